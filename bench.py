@@ -1,0 +1,456 @@
+#!/usr/bin/env python
+"""Benchmark: solves/s of the HODLR direct solve on B200.
+
+Workload (default): N = 262144 unknowns, dense leaves of 512 rows (512 leaves,
+9 levels), rank 64 at every level, 16 right-hand sides; seeded synthetic
+system (leaf blocks G/sqrt(512) + 2I, U/V iid Gaussian rescaled so every
+off-diagonal block has spectral norm 0.5, b iid N(0,1)), generated on the
+device.  One step = one solve of that system with its whole RHS block:
+
+  value     mixed precision: FP32 leaf LU, FP32 reduce/broadcast, FP64 node
+            LU, FP64 HODLR-matvec residual and FP64 refinement sweeps until
+            max_j ||b_j - A x_j|| / ||b_j|| <= 1e-12 (factor + refinement
+            inside every step)
+  fp64_gpu  the plain FP64 path (the fused factor+solve of the reference's
+            bfs_solve), same system, timed the same way
+  e2e       `value`'s solve through the public API with the system in pinned
+            host memory: H2D of D, U, V, b and D2H of x inside every step
+  --impl reference: the CPU oracle (a restatement of the reference's
+            Legion+LAPACK path with OpenBLAS, all host threads) on the same
+            workload, printed as the reference arm.
+
+Inputs are ~3.5 GB, far above the 126 MB L2, so no explicit flush is needed.
+Multi-GPU (torchrun): every rank solves its own system (replicas, weak
+scaling, no collective on the data path); value = total solves / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "n262144": dict(N=262144, leaf=512, rank=64, nrhs=16),   # the metric's system
+    "n65536": dict(N=65536, leaf=512, rank=50, nrhs=8),
+    "n4096": dict(N=4096, leaf=256, rank=30, nrhs=1),
+    "n1048576": dict(N=1048576, leaf=512, rank=100, nrhs=32),
+}
+METRIC = "solves/s at N=2^18,r=64: mixed+batched vs plain FP64 GPU @relres<=1e-12"
+TOL = 1e-12
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work of one fused solve (per phase), from the tree
+# ---------------------------------------------------------------------------
+
+def work_model(tree: np.ndarray, m: int):
+    """Flops and compulsory bytes (FP64 words x 8) of one fused factor+solve."""
+    nrow, ncol, rb, cb, lc, rc, par, dep, vnc, leaf = (tree[:, i] for i in range(10))
+    w = dict(getrf=0.0, getrs=0.0, reduce=0.0, node=0.0, broadcast=0.0)
+    for i in range(tree.shape[0]):
+        if leaf[i]:
+            n = float(nrow[i])
+            c = float(cb[i] + ncol[i])
+            w["getrf"] += 2.0 / 3.0 * n ** 3
+            w["getrs"] += 2.0 * n * n * c
+            continue
+        a, b = lc[i], rc[i]
+        cw = float(cb[a])
+        r0, r1 = float(ncol[a]), float(ncol[b])
+        for ch in (a, b):
+            w["reduce"] += 2.0 * nrow[ch] * vnc[ch] * (cb[ch] + ncol[ch])
+            w["broadcast"] += 2.0 * nrow[ch] * ncol[ch] * cw
+        w["node"] += 2 * r0 * r1 * r0 + 2.0 / 3.0 * r0 ** 3 + 2 * r0 * r0 * cw + 4 * r0 * r1 * cw
+    return w
+
+
+def phase_bytes(tree: np.ndarray, m: int, word: int):
+    """Compulsory bytes per phase of one fused solve in `word`-byte arithmetic."""
+    nrow, ncol, rb, cb, lc, rc, par, dep, vnc, leaf = (tree[:, i] for i in range(10))
+    b = dict(getrf=0.0, getrs=0.0, reduce=0.0, node=0.0, broadcast=0.0)
+    for i in range(tree.shape[0]):
+        if leaf[i]:
+            n = float(nrow[i])
+            c = float(cb[i] + ncol[i])
+            b["getrf"] += 2 * n * n * word          # read D, write LU
+            b["getrs"] += (n * n + 2 * n * c) * word  # read LU, read+write X
+            continue
+        a, bb = lc[i], rc[i]
+        cw = float(cb[a])
+        for ch in (a, bb):
+            b["reduce"] += nrow[ch] * (vnc[ch] + cb[ch] + ncol[ch]) * word
+            b["broadcast"] += nrow[ch] * (ncol[ch] + 2 * cw) * word
+    return b
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return dict(hbm=float(p["hbm_gbs"]), bf16=float(p["bf16_tflops"]),
+                    sm_mhz=float(p.get("sm_max_mhz", 1965.0)), src="measured")
+    return dict(hbm=6650.0, bf16=1590.0, sm_mhz=1965.0, src="fallback")
+
+
+def simt_peak_tflops(word: int, sm_mhz: float) -> float:
+    """Nominal SIMT FMA peak: 148 SMs x (128 FP32 | 64 FP64) FMA/clk x 2."""
+    lanes = 128 if word == 4 else 64
+    return 148 * lanes * 2 * sm_mhz * 1e6 / 1e12
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_system(fs, cfg, seed):
+    h = fs.HodlrMatrix(cfg["nrhs"], cfg["N"], cfg["rank"], cfg["leaf"]).create_tree()
+    h.init_gaussian(seed, 0.5)
+    return h
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU oracle (restated reference path) on the host cores
+# ---------------------------------------------------------------------------
+
+def run_reference(args, cfg):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import refcpu as R
+    threads = os.cpu_count() or 1
+    s = R.gaussian_system(cfg["N"], cfg["nrhs"], cfg["rank"], cfg["leaf"], seed=args.seed)
+    R.lib().ref_set_blas_threads(1)
+    for _ in range(args.warmup):
+        R.bfs_solve(s, nthreads=threads)
+    t0 = time.perf_counter()
+    rr = 0.0
+    for _ in range(args.steps):
+        X, _ = R.bfs_solve(s, nthreads=threads)
+    dt = time.perf_counter() - t0
+    rr = R.relres(s, X[:, : cfg["nrhs"]])
+    v = args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Gaussian HODLR system, numpy PCG64)",
+        "config": {"workload": f"hodlr_solve N={cfg['N']} leaf={cfg['leaf']} r={cfg['rank']} "
+                               f"m={cfg['nrhs']}", **cfg, "relres": rr},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full fused FP64 solves (oracle/refcpu.c: "
+                                   "restated task bodies + BFS walk, OpenBLAS dgesv/dgemm, "
+                                   "one OpenMP task per leaf/node of a level)"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="n262144", choices=sorted(CONFIGS))
+    ap.add_argument("--seed", type=int, default=1245667)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-solves", type=int, default=2)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        return run_reference(args, cfg)
+
+    import torch
+    import fastsolver_b200 as fs
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    stream = torch.cuda.current_stream()
+    h = make_system(fs, cfg, args.seed + rank)
+    tree = h.tree_nodes()
+    solver = fs.FastSolver()
+
+    def mixed_step():
+        it, rr = solver.solve_refined(h, fs.PREC_MIXED, tol=TOL, maxiter=10, stream=stream)
+        return it, rr
+
+    def fp64_step():
+        solver.bfs_solve(h, sync=False, stream=stream)
+
+    # ---- warm-up
+    for _ in range(args.warmup):
+        mixed_step()
+    torch.cuda.synchronize()
+
+    # ---- timed: mixed precision (the metric's value)
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    fs.reset_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters, rrs = [], []
+    e0.record(stream)
+    for _ in range(args.steps):
+        it, rr = mixed_step()
+        iters.append(it)
+        rrs.append(rr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = fs.launch_count()
+    clk = clocks.stop()
+    ms_mixed = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    barrier()
+
+    # ---- timed: plain FP64 path
+    for _ in range(args.warmup):
+        fp64_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        fp64_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_fp64 = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    rr_fp64 = h.relres(stream=stream)
+
+    # ---- per-phase device time (separate, event-bracketed pass)
+    h.set_profiling(True)
+    mixed_step()
+    ph_mixed = h.phase_times(reset=True)
+    fp64_step()
+    torch.cuda.synchronize()
+    ph_fp64 = h.phase_times(reset=True)
+    h.set_profiling(False)
+
+    # ---- end to end through the public API from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        D, U, V, B = h.get_matrix()
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a.T)).pin_memory()  # noqa: E731
+        Dp, Up, Vp, Bp = pin(D), pin(U), pin(V), pin(B)
+        xout = torch.empty((cfg["nrhs"], cfg["N"]), dtype=torch.float64).pin_memory()
+        N = cfg["N"]
+        from fastsolver_b200._lib import call
+        import ctypes
+
+        def e2e_step():
+            call("hodlr_set_matrix", h.handle, Dp.data_ptr(), N, Up.data_ptr(), N,
+                 Vp.data_ptr(), N, 1, stream.cuda_stream)
+            call("hodlr_set_rhs", h.handle, Bp.data_ptr(), N, 1, stream.cuda_stream)
+            mixed_step()
+            call("hodlr_get_solution", h.handle, xout.data_ptr(), N, 1, stream.cuda_stream)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        ksteps = max(2, min(args.steps, 5))
+        e0.record(stream)
+        for _ in range(ksteps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = max_over_ranks(e0.elapsed_time(e1) / ksteps)
+        h2d = (Dp.numel() + Up.numel() + Vp.numel() + Bp.numel()) * 8
+        e2e = {"value": ws * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(xout.numel() * 8), "ms_per_step": ms_e2e,
+               "steps": ksteps}
+
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel and of the whole solve
+    pk = peaks()
+    m = cfg["nrhs"]
+    W = work_model(tree, m)
+    B4 = phase_bytes(tree, m, 4)
+    B8 = phase_bytes(tree, m, 8)
+    fp32_peak = simt_peak_tflops(4, pk["sm_mhz"])
+    fp64_peak = simt_peak_tflops(8, pk["sm_mhz"])
+    phase_flops = {"getrf": W["getrf"], "getrs": W["getrs"], "reduce": W["reduce"],
+                   "node_apply": W["node"], "broadcast": W["broadcast"]}
+    # the factor pass of the mixed solve carries b, so its per-phase work equals the
+    # fused model; refinement sweeps add getrs/reduce/broadcast launches on m columns
+    dom = max(("getrf", "getrs", "reduce", "broadcast"),
+              key=lambda k: ph_mixed[k][0])
+    ms_dom, n_dom = ph_mixed[dom]
+    # the dominant phase's first launch is the factor pass: time one launch of it
+    h.set_profiling(True)
+    solver.factor(h, fs.PREC_MIXED, stream=stream)
+    ph_f = h.phase_times(reset=True)
+    h.set_profiling(False)
+    ms_one, n_one = ph_f[dom]
+    per_launch_ms = ms_one / max(n_one, 1)
+    flops_per_launch = phase_flops[dom] / (1 if dom in ("getrf", "getrs") else max(n_one, 1))
+    achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32-simt", "kernel": {"getrf": "getrf_kernel<float>",
+                                                "getrs": "getrs_kernel<float>",
+                                                "reduce": "gemm_items_kernel<float> (reduce)",
+                                                "broadcast": "gemm_items_kernel<float> (bcast)"}[dom],
+                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": None,
+                "peak_note": f"nominal FP32 FMA peak 148 SM x 128 x 2 x {pk['sm_mhz']:.0f} MHz"}
+
+    def solve_frac(ms, word, peak_tf):
+        Bx = B4 if word == 4 else B8
+        t = 0.0
+        for k in ("getrf", "getrs", "reduce", "broadcast"):
+            t += max(W[k] / (peak_tf * 1e12), Bx[k] / (pk["hbm"] * 1e9))
+        t += W["node"] / (fp64_peak * 1e12)
+        return t * 1e3 / ms
+
+    total_flops = sum(W.values())
+    cpu = None
+    if not args.no_cpu_baseline and ws == 1:
+        from oracle import refcpu as R
+        D, U, V, B = h.get_matrix()
+        s = R.System(tree, D, U, V, B)
+        threads = os.cpu_count() or 1
+        R.lib().ref_set_blas_threads(1)
+        t0 = time.perf_counter()
+        for _ in range(args.cpu_solves):
+            Xc, _ = R.bfs_solve(s, nthreads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": args.cpu_solves / dt, "unit": "solves/s", "cores": threads,
+               "kind": "port",
+               "sample": f"{args.cpu_solves} full fused FP64 solves of the same system "
+                         "(oracle/refcpu.c, OpenBLAS, one OpenMP task per leaf/node)"}
+
+    value = ws * 1e3 / ms_mixed
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded Gaussian HODLR system generated on the device, Philox4x32-10)",
+        "config": {"workload": f"hodlr_solve N={cfg['N']} leaf={cfg['leaf']} r={cfg['rank']} "
+                               f"m={cfg['nrhs']} mixed+refine to relres<=1e-12",
+                   **cfg, "levels": int(tree[:, 7].max()), "l2": "inputs 3.5 GB > L2",
+                   "parallelism": f"replicas x{ws}"},
+        "relres_max": float(max(rrs)), "refine_sweeps": iters,
+        "fp64_gpu": {"value": ws * 1e3 / ms_fp64, "unit": "solves/s", "ms_per_step": ms_fp64,
+                     "relres": rr_fp64,
+                     "roofline_frac": solve_frac(ms_fp64, 8, fp64_peak),
+                     "tflops": total_flops / (ms_fp64 * 1e-3) / 1e12},
+        "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "mixed_roofline_frac": solve_frac(ms_mixed, 4, fp32_peak),
+        "gflop_per_solve": total_flops / 1e9,
+        "roofline": roofline,
+        "phases_ms": {"mixed": {k: round(v[0], 4) for k, v in ph_mixed.items()},
+                      "fp64": {k: round(v[0], 4) for k, v in ph_fp64.items()}},
+        "peaks": {"hbm_gbs": pk["hbm"], "src": pk["src"], "fp64_tflops_nominal": fp64_peak,
+                  "fp32_tflops_nominal": fp32_peak},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,766 @@
+// capi.cu -- the extern "C" entry points declared in include/hodlr_gpu.h.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "gemm_simt.cuh"
+#include "leaf.cuh"
+#include "node.cuh"
+#include "solver.h"
+#include "util.cuh"
+
+namespace hodlr {
+
+namespace {
+thread_local long long g_launches = 0;
+}
+
+void count_launch() { ++g_launches; }
+
+}  // namespace hodlr
+
+using namespace hodlr;
+
+struct hodlr_system_s {
+  System sys;
+};
+
+namespace {
+
+// Runs `f` and maps library exceptions to status codes.
+template <typename F>
+int guarded(F &&f) {
+  try {
+    return f();
+  } catch (const CudaError &e) {
+    return e.err == cudaErrorMemoryAllocation ? HODLR_ERR_NOMEM : HODLR_ERR_CUDA;
+  } catch (const std::bad_alloc &) {
+    return HODLR_ERR_NOMEM;
+  }
+}
+
+int device_ok() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return HODLR_ERR_CUDA;
+  }
+  return 0;
+}
+
+// Small stream-ordered device scratch for single-call task bodies.
+struct StreamScratch {
+  void *p = nullptr;
+  cudaStream_t s;
+  explicit StreamScratch(size_t bytes, cudaStream_t st) : s(st) {
+    HODLR_CUDA_TRY(cudaMallocAsync(&p, bytes, s));
+  }
+  ~StreamScratch() {
+    if (p) cudaFreeAsync(p, s);
+  }
+};
+
+int finish_info(int *info_user, int *info_dev, cudaStream_t s) {
+  if (info_user) return 0;
+  int h = 0;
+  HODLR_CUDA_TRY(cudaMemcpyAsync(&h, info_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+  HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+  return h;
+}
+
+}  // namespace
+
+extern "C" {
+
+long long hodlr_launch_count(void) { return g_launches; }
+void hodlr_reset_launch_count(void) { g_launches = 0; }
+
+const char *hodlr_status_string(int status) {
+  switch (status) {
+    case HODLR_OK: return "ok";
+    case HODLR_ERR_CUDA: return "CUDA runtime error or no CUDA device";
+    case HODLR_ERR_NOMEM: return "device allocation failed";
+    case HODLR_ERR_STATE: return "call out of order";
+    case HODLR_ERR_NOCONV: return "refinement did not reach the tolerance";
+    case HODLR_ERR_TIMEOUT: return "bounded device wait gave up";
+    case HODLR_ERR_UNSUPPORTED: return "unsupported size or option";
+    default: break;
+  }
+  if (status > 0) return "zero pivot (LAPACK-style INFO)";
+  return "invalid argument";
+}
+
+// ---------------------------------------------------------------------------
+// task bodies
+// ---------------------------------------------------------------------------
+
+int hodlr_leaf_solve(int n, int nrhs, double *D, int ldd, double *X, int ldx, int *ipiv,
+                     int *info, hodlr_stream_t stream) {
+  if (n < 0) return -1;
+  if (nrhs < 0) return -2;
+  if (!D && n > 0) return -3;
+  if (ldd < (n > 1 ? n : 1)) return -4;
+  if (!X && n > 0 && nrhs > 0) return -5;
+  if (ldx < (n > 1 ? n : 1)) return -6;
+  if (!ipiv && n > 0) return -7;
+  if (n > 1024) return HODLR_ERR_UNSUPPORTED;
+  if (int e = device_ok()) return e;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    if (n == 0) return 0;
+    StreamScratch scr(sizeof(int), s);
+    int *info_dev = info ? info : static_cast<int *>(scr.p);
+    LeafTask<double> tk{};
+    tk.D = D; tk.ldd = ldd; tk.X = X; tk.ldx = ldx; tk.ipiv = ipiv; tk.perm = nullptr;
+    tk.n = n; tk.nrhs = nrhs; tk.info_slot = 0;
+    launch_getrf<double>(nullptr, tk, 1, n, info_dev, s);
+    if (nrhs > 0) launch_getrs<double>(nullptr, tk, 1, n, nrhs, s);
+    return finish_info(info, info_dev, s);
+  });
+}
+
+int hodlr_leaf_solve_batched(int count, const hodlr_leaf_desc *descs, int max_n, int max_nrhs,
+                             int *info, hodlr_stream_t stream) {
+  if (count < 0) return -1;
+  if (!descs && count > 0) return -2;
+  if (max_n < 0 || max_n > 1024) return max_n < 0 ? -3 : HODLR_ERR_UNSUPPORTED;
+  if (max_nrhs < 0) return -4;
+  if (!info && count > 0) return -5;
+  if (int e = device_ok()) return e;
+  static_assert(sizeof(hodlr_leaf_desc) == sizeof(LeafTask<double>) - 2 * sizeof(int),
+                "descriptor layout");
+  return guarded([&]() -> int {
+    if (count == 0) return 0;
+    cudaStream_t s = as_stream(stream);
+    // hodlr_leaf_desc has no info_slot: expand into LeafTask on the device
+    std::vector<hodlr_leaf_desc> h(count);
+    HODLR_CUDA_TRY(cudaMemcpyAsync(h.data(), descs, sizeof(hodlr_leaf_desc) * count,
+                                   cudaMemcpyDeviceToHost, s));
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<LeafTask<double>> t(count);
+    for (int i = 0; i < count; ++i) {
+      t[i].D = h[i].D; t[i].X = h[i].X; t[i].ipiv = h[i].ipiv; t[i].perm = h[i].perm;
+      t[i].ldd = h[i].ldd; t[i].ldx = h[i].ldx; t[i].n = h[i].n; t[i].nrhs = h[i].nrhs;
+      t[i].info_slot = i;
+      if (h[i].n > max_n || h[i].nrhs > max_nrhs || h[i].ldd < h[i].n || h[i].ldx < h[i].n)
+        return -2;
+    }
+    StreamScratch scr(sizeof(LeafTask<double>) * count, s);
+    HODLR_CUDA_TRY(cudaMemcpyAsync(scr.p, t.data(), sizeof(LeafTask<double>) * count,
+                                   cudaMemcpyHostToDevice, s));
+    LeafTask<double> none{};
+    auto *tp = static_cast<LeafTask<double> *>(scr.p);
+    launch_getrf<double>(tp, none, count, max_n, info, s);
+    launch_getrs<double>(tp, none, count, max_n, max_nrhs, s);
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  });
+}
+
+int hodlr_gemm_reduce(double alpha, int k, int r, int ncol, const double *V, int ldv,
+                      const double *U, int ldu, int col_beg, double *W, int ldw,
+                      hodlr_stream_t stream) {
+  if (k < 0) return -2;
+  if (r < 0) return -3;
+  if (ncol < 0) return -4;
+  if (!V && k > 0 && r > 0) return -5;
+  if (ldv < (k > 1 ? k : 1)) return -6;
+  if (!U && k > 0 && ncol > 0) return -7;
+  if (ldu < (k > 1 ? k : 1)) return -8;
+  if (col_beg < 0) return -9;
+  if (!W && r > 0 && ncol > 0) return -10;
+  if (ldw < (r > 1 ? r : 1)) return -11;
+  if (int e = device_ok()) return e;
+  return guarded([&]() -> int {
+    if (r == 0 || ncol == 0) return 0;
+    cudaStream_t s = as_stream(stream);
+    // split K into row chunks: partials in scratch, then W += sum (fixed order)
+    const int chunk = 4096;
+    const int nsl = k > 0 ? cdiv(k, chunk) : 0;
+    if (nsl == 0) return 0;
+    std::vector<GemmItem<double, double>> it(nsl);
+    std::vector<GemmSeg<double>> sg(nsl);
+    const size_t slot = (size_t)r * ncol;
+    StreamScratch part(sizeof(double) * slot * nsl, s);
+    double *pp = static_cast<double *>(part.p);
+    for (int q = 0; q < nsl; ++q) {
+      const int rb = q * chunk, rows = std::min(chunk, k - rb);
+      sg[q] = GemmSeg<double>{V + rb, U + rb + (long long)col_beg * ldu, ldv, ldu, rows, 0};
+      it[q] = GemmItem<double, double>{pp + q * slot, nullptr, r, 0, r, ncol, q, 1};
+    }
+    StreamScratch desc(sizeof(GemmItem<double, double>) * nsl + sizeof(GemmSeg<double>) * nsl +
+                           2 * sizeof(GemmItem<double, double>) + sizeof(SumTask<double>) + 256,
+                       s);
+    auto *di = static_cast<GemmItem<double, double> *>(desc.p);
+    auto *ds = reinterpret_cast<GemmSeg<double> *>(di + nsl);
+    HODLR_CUDA_TRY(cudaMemcpyAsync(di, it.data(), sizeof(it[0]) * nsl, cudaMemcpyHostToDevice, s));
+    HODLR_CUDA_TRY(cudaMemcpyAsync(ds, sg.data(), sizeof(sg[0]) * nsl, cudaMemcpyHostToDevice, s));
+    launch_gemm_items<double, double, double>(di, ds, nsl, r, ncol, true, alpha, 0.0, s);
+    // W += fixed-order sum of the partials
+    SumTask<double> st{};
+    StreamScratch tmp(sizeof(double) * slot, s);
+    st.dst = static_cast<double *>(tmp.p);
+    st.src = pp;
+    st.len = (long long)slot;
+    st.stride = (long long)slot;
+    st.nslots = nsl;
+    auto *dst = reinterpret_cast<SumTask<double> *>(ds + nsl);
+    HODLR_CUDA_TRY(cudaMemcpyAsync(dst, &st, sizeof(st), cudaMemcpyHostToDevice, s));
+    launch_sum_slots<double>(dst, 1, st.len, s);
+    launch_add2d<double>(W, ldw, static_cast<double *>(tmp.p), r, r, ncol, s);
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  });
+}
+
+static int node_solve_common(int form, int r0, int r1, int c, const double *V0Tu0, int ld00,
+                             const double *V1Tu1, int ld11, double *V0Td0, int ld0d,
+                             double *V1Td1, int ld1d, int *info, hodlr_stream_t stream) {
+  if (r0 <= 0) return -1;
+  if (r1 <= 0) return -2;
+  if (c < 0) return -3;
+  if (!V0Tu0) return -4;
+  if (ld00 < r1) return -5;
+  if (!V1Tu1) return -6;
+  if (ld11 < r0) return -7;
+  if (!V0Td0 && c > 0) return -8;
+  if (ld0d < r1) return -9;
+  if (!V1Td1 && c > 0) return -10;
+  if (ld1d < r0) return -11;
+  const int s_ = form == 0 ? r0 : r0 + r1;
+  if (form == 1 && r0 != r1) return HODLR_ERR_UNSUPPORTED;
+  if (s_ > kMaxNodeS) return HODLR_ERR_UNSUPPORTED;
+  if (int e = device_ok()) return e;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    const size_t need = sizeof(double) * ((size_t)s_ * s_ + 2 * (size_t)r0 * r1) +
+                        sizeof(int) * (s_ + 8) + sizeof(NodeTask<double, double>) + 1024;
+    StreamScratch scr(need, s);
+    char *base = static_cast<char *>(scr.p);
+    auto *task = reinterpret_cast<NodeTask<double, double> *>(base);
+    double *S_lu = reinterpret_cast<double *>(base + 256);
+    double *VTu0 = S_lu + (size_t)s_ * s_;
+    double *VTu1 = VTu0 + (size_t)r0 * r1;
+    int *piv = reinterpret_cast<int *>(VTu1 + (size_t)r0 * r1);
+    int *info_dev = info ? info : piv + s_;
+    NodeTask<double, double> k{};
+    k.W0d = V0Td0; k.W0u = V0Tu0; k.W1d = V1Td1; k.W1u = V1Tu1;
+    k.w0_stride = k.w1_stride = 0;
+    k.ldw0d = ld0d; k.ldw0u = ld00; k.ldw1d = ld1d; k.ldw1u = ld11;
+    k.np0 = k.np1 = 1;
+    k.r0 = r0; k.r1 = r1; k.c = c;
+    // outputs in place: form 0 writes eta0 over V1Td1, eta1 over V0Td0
+    // (fast_solver.cc:238-240); form 1 eta0 over V0Td0, eta1 over V1Td1.
+    if (form == 0) { k.eta0 = V1Td1; k.ld_eta0 = ld1d; k.eta1 = V0Td0; k.ld_eta1 = ld0d; }
+    else { k.eta0 = V0Td0; k.ld_eta0 = ld0d; k.eta1 = V1Td1; k.ld_eta1 = ld1d; }
+    k.S_lu = S_lu; k.S_piv = piv; k.VTu0 = VTu0; k.VTu1 = VTu1;
+    k.info_slot = 0;
+    HODLR_CUDA_TRY(cudaMemcpyAsync(task, &k, sizeof(k), cudaMemcpyHostToDevice, s));
+    launch_node_factor<double, double>(task, 1, s_, form, info_dev, s);
+    if (c > 0) launch_node_apply<double, double>(task, 1, s_, r0 + r1, c, form, s);
+    int rc = finish_info(info, info_dev, s);
+    if (info) HODLR_CUDA_TRY(cudaStreamSynchronize(s));  // scratch lifetime
+    return rc;
+  });
+}
+
+int hodlr_node_lu_solve(int r0, int r1, int c, const double *V0Tu0, int ld00,
+                        const double *V1Tu1, int ld11, double *V0Td0, int ld0d, double *V1Td1,
+                        int ld1d, int *info, hodlr_stream_t stream) {
+  return node_solve_common(0, r0, r1, c, V0Tu0, ld00, V1Tu1, ld11, V0Td0, ld0d, V1Td1, ld1d,
+                           info, stream);
+}
+
+int hodlr_node_schur2_solve(int r0, int r1, int c, const double *V0Tu0, int ld00,
+                            const double *V1Tu1, int ld11, double *V0Td0, int ld0d,
+                            double *V1Td1, int ld1d, int *info, hodlr_stream_t stream) {
+  return node_solve_common(1, r0, r1, c, V0Tu0, ld00, V1Tu1, ld11, V0Td0, ld0d, V1Td1, ld1d,
+                           info, stream);
+}
+
+int hodlr_gemm_broadcast(double alpha, double beta, int k, int r, int c, double *X, int ldx,
+                         int u_col_beg, const double *eta, int lde, int d_col_beg,
+                         hodlr_stream_t stream) {
+  if (k < 0) return -3;
+  if (r < 0) return -4;
+  if (c < 0) return -5;
+  if (!X && k > 0) return -6;
+  if (ldx < (k > 1 ? k : 1)) return -7;
+  if (u_col_beg < 0) return -8;
+  if (!eta && r > 0 && c > 0) return -9;
+  if (lde < (r > 1 ? r : 1)) return -10;
+  if (d_col_beg < 0) return -11;
+  if (!(u_col_beg + r <= d_col_beg || d_col_beg + c <= u_col_beg)) return -11;
+  if (int e = device_ok()) return e;
+  return guarded([&]() -> int {
+    if (k == 0 || c == 0) return 0;
+    cudaStream_t s = as_stream(stream);
+    GemmSeg<double> sg{X + (long long)u_col_beg * ldx, eta, ldx, lde, r, 0};
+    double *Cp = X + (long long)d_col_beg * ldx;
+    GemmItem<double, double> it{Cp, Cp, ldx, ldx, k, c, 0, 1};
+    StreamScratch scr(sizeof(sg) + sizeof(it) + 64, s);
+    auto *di = static_cast<GemmItem<double, double> *>(scr.p);
+    auto *ds = reinterpret_cast<GemmSeg<double> *>(di + 1);
+    HODLR_CUDA_TRY(cudaMemcpyAsync(di, &it, sizeof(it), cudaMemcpyHostToDevice, s));
+    HODLR_CUDA_TRY(cudaMemcpyAsync(ds, &sg, sizeof(sg), cudaMemcpyHostToDevice, s));
+    launch_gemm_items<double, double, double>(di, ds, 1, k, c, false, alpha, beta, s);
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  });
+}
+
+// ---------------------------------------------------------------------------
+// handle API
+// ---------------------------------------------------------------------------
+
+int hodlr_build_tree(int N, int nrhs, int rank, int threshold, int *out, int cap) {
+  Tree t;
+  const int rc = build_tree(N, nrhs, rank, threshold, t);
+  if (rc < 0) return rc;
+  if (!out || cap < (int)t.nodes.size()) return -6;
+  std::memcpy(out, t.nodes.data(), sizeof(Node) * t.nodes.size());
+  return (int)t.nodes.size();
+}
+
+int hodlr_create(hodlr_system *out, int N, int nrhs, int rank, int threshold) {
+  if (!out) return -1;
+  *out = nullptr;
+  if (N <= 0) return -2;
+  if (nrhs <= 0) return -3;
+  if (rank <= 0) return -4;
+  if (threshold <= 0) return -5;
+  if (rank > kMaxNodeS) return HODLR_ERR_UNSUPPORTED;
+  if (int e = device_ok()) return e;
+  auto *h = new (std::nothrow) hodlr_system_s;
+  if (!h) return HODLR_ERR_NOMEM;
+  int rc = guarded([&]() -> int {
+    int t = h->sys.init(N, nrhs, rank, threshold);
+    if (t < 0) return t - 1;  // -1..-4 of build_tree -> argument positions 2..5
+    if (h->sys.nmax > 1024) return HODLR_ERR_UNSUPPORTED;
+    return 0;
+  });
+  if (rc != 0) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return 0;
+}
+
+int hodlr_destroy(hodlr_system sys) {
+  if (!sys) return -1;
+  delete sys;
+  return 0;
+}
+
+int hodlr_tree_info(hodlr_system h, int *nnodes, int *max_depth, int *nleaves, int *ncols,
+                    int *max_leaf) {
+  if (!h) return -1;
+  const Tree &t = h->sys.tree;
+  if (nnodes) *nnodes = (int)t.nodes.size();
+  if (max_depth) *max_depth = t.max_depth;
+  if (nleaves) *nleaves = (int)t.leaves.size();
+  if (ncols) *ncols = t.ncols;
+  if (max_leaf) *max_leaf = t.max_leaf;
+  return 0;
+}
+
+int hodlr_tree_nodes(hodlr_system h, int *out, int cap) {
+  if (!h) return -1;
+  const Tree &t = h->sys.tree;
+  if (!out || cap < (int)t.nodes.size()) return -2;
+  std::memcpy(out, t.nodes.data(), sizeof(Node) * t.nodes.size());
+  return 0;
+}
+
+static int copy2d(double *dst, long long ldd, const double *src, long long lds, long long rows,
+                  long long cols, int host, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return 0;
+  HODLR_CUDA_TRY(cudaMemcpy2DAsync(dst, sizeof(double) * ldd, src, sizeof(double) * lds,
+                                   sizeof(double) * rows, cols,
+                                   host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+  return 0;
+}
+
+int hodlr_set_matrix(hodlr_system h, const double *D, long long ldd, const double *U,
+                     long long ldu, const double *V, long long ldv, int host,
+                     hodlr_stream_t stream) {
+  if (!h) return -1;
+  System &S = h->sys;
+  if (D && ldd < S.N) return -3;
+  if (U && ldu < S.N) return -5;
+  if (V && ldv < S.N) return -7;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    if (D) copy2d(S.D.p, S.N, D, ldd, S.N, S.nmax, host, s);
+    if (U) copy2d(S.U.p, S.N, U, ldu, S.N, S.vc, host, s);
+    if (V) copy2d(S.V.p, S.N, V, ldv, S.N, S.vc, host, s);
+    if (host) HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    S.factored = -1;
+    return 0;
+  });
+}
+
+int hodlr_set_rhs(hodlr_system h, const double *B, long long ldb, int host,
+                  hodlr_stream_t stream) {
+  if (!h) return -1;
+  System &S = h->sys;
+  if (!B) return -2;
+  if (ldb < S.N) return -3;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    copy2d(S.B.p, S.N, B, ldb, S.N, S.m, host, s);
+    if (host) HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  });
+}
+
+int hodlr_get_matrix(hodlr_system h, double *D, long long ldd, double *U, long long ldu,
+                     double *V, long long ldv, double *B, long long ldb, int host,
+                     hodlr_stream_t stream) {
+  if (!h) return -1;
+  System &S = h->sys;
+  if (D && ldd < S.N) return -3;
+  if (U && ldu < S.N) return -5;
+  if (V && ldv < S.N) return -7;
+  if (B && ldb < S.N) return -9;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    const cudaMemcpyKind k = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    auto out = [&](double *dst, long long ld, const double *src, long long cols) {
+      if (!dst || cols <= 0) return;
+      HODLR_CUDA_TRY(cudaMemcpy2DAsync(dst, sizeof(double) * ld, src, sizeof(double) * S.N,
+                                       sizeof(double) * S.N, cols, k, s));
+    };
+    out(D, ldd, S.D.p, S.nmax);
+    out(U, ldu, S.U.p, S.vc);
+    out(V, ldv, S.V.p, S.vc);
+    out(B, ldb, S.B.p, S.m);
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  });
+}
+
+static std::vector<int2> leaf_ranges(const Tree &t) {
+  std::vector<int2> v;
+  for (int id : t.leaves) v.push_back(make_int2(t.nodes[id].row_beg, t.nodes[id].nrow));
+  return v;
+}
+
+int hodlr_init_circulant(hodlr_system h, double diag, hodlr_stream_t stream) {
+  if (!h) return -1;
+  return guarded([&]() -> int {
+    System &S = h->sys;
+    cudaStream_t s = as_stream(stream);
+    DevBuf<int2> lv;
+    lv.upload(leaf_ranges(S.tree));
+    HODLR_CUDA_TRY(cudaMemsetAsync(S.D.p, 0, sizeof(double) * (size_t)S.N * S.nmax, s));
+    launch_circulant_k(lv.p, (int)S.tree.leaves.size(), S.nmax, S.D.p, S.N, S.r, diag, s);
+    launch_circulant_uv(S.U.p, S.N, S.V.p, S.N, S.N, S.vc, S.r, s);
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    S.factored = -1;
+    return 0;
+  });
+}
+
+int hodlr_init_rhs_drand48(hodlr_system h, long seed, hodlr_stream_t stream) {
+  if (!h) return -1;
+  return guarded([&]() -> int {
+    System &S = h->sys;
+    cudaStream_t s = as_stream(stream);
+    DevBuf<int2> lv;
+    lv.upload(leaf_ranges(S.tree));
+    launch_drand48(lv.p, (int)S.tree.leaves.size(), S.B.p, S.N, S.m, seed, s);
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  });
+}
+
+int hodlr_init_gaussian(hodlr_system h, unsigned long long seed, double offdiag_norm,
+                        hodlr_stream_t stream) {
+  if (!h) return -1;
+  if (!(offdiag_norm > 0.0)) return -3;
+  return guarded([&]() -> int {
+    System &S = h->sys;
+    const Tree &t = S.tree;
+    cudaStream_t s = as_stream(stream);
+    const long long N = S.N;
+    const int m = S.m;
+    HODLR_CUDA_TRY(cudaMemsetAsync(S.D.p, 0, sizeof(double) * (size_t)N * S.nmax, s));
+    for (size_t q = 0; q < t.leaves.size(); ++q) {
+      const Node &n = t.nodes[t.leaves[q]];
+      launch_gauss_fill(S.D.p + n.row_beg, N, n.nrow, n.nrow, seed, (unsigned)(1 + q),
+                        1.0 / std::sqrt((double)n.nrow), 2.0, 0, s);
+    }
+    const unsigned base = (unsigned)(1 + t.leaves.size());
+    for (size_t i = 1; i < t.nodes.size(); ++i) {
+      const Node &c = t.nodes[i];
+      const double sc = 1.0 / std::sqrt((double)c.ncol * c.nrow);
+      launch_gauss_fill(S.U.p + c.row_beg + (long long)(c.col_beg - m) * N, N, c.nrow, c.ncol,
+                        seed, base + 2 * (unsigned)i, sc, 0.0, 0, s);
+      launch_gauss_fill(S.V.p + c.row_beg + (long long)(c.col_beg - m) * N, N, c.nrow, c.vncol,
+                        seed, base + 2 * (unsigned)i + 1, sc, 0.0, 0, s);
+    }
+    launch_gauss_fill(S.B.p, N, N, m, seed, base + 2 * (unsigned)t.nodes.size() + 2, 1.0, 0.0, 0,
+                      s);
+    // Rescale each off-diagonal block U_c V_s^T to spectral norm offdiag_norm:
+    // ||U V^T||_2^2 = lambda_max((U^T U)(V^T V)); Grams via chunked reduces.
+    std::vector<int> ids;
+    for (size_t i = 1; i < t.nodes.size(); ++i) ids.push_back((int)i);
+    const int r = S.r;
+    const int chunk = 4096;
+    std::vector<GemmItem<double, double>> it;
+    std::vector<GemmSeg<double>> sg;
+    std::vector<SumTask<double>> st;
+    size_t nslot_total = 0;
+    for (int i : ids) nslot_total += 2 * (size_t)cdiv(t.nodes[i].nrow, chunk);
+    DevBuf<double> part, gram;
+    part.ensure(nslot_total * r * r);
+    gram.ensure(2 * ids.size() * (size_t)r * r);
+    size_t slot = 0;
+    for (size_t q = 0; q < ids.size(); ++q) {
+      const Node &c = t.nodes[ids[q]];
+      for (int which = 0; which < 2; ++which) {
+        const double *A = (which == 0 ? S.U.p : S.V.p) + c.row_beg + (long long)(c.col_beg - m) * N;
+        const int ns = cdiv(c.nrow, chunk);
+        SumTask<double> sk{};
+        sk.dst = gram.p + (2 * q + which) * (size_t)r * r;
+        sk.src = part.p + slot * r * r;
+        sk.len = (long long)r * r;
+        sk.stride = (long long)r * r;
+        sk.nslots = ns;
+        st.push_back(sk);
+        for (int z = 0; z < ns; ++z) {
+          const int rb = z * chunk, rows = std::min(chunk, c.nrow - rb);
+          sg.push_back(GemmSeg<double>{A + rb, A + rb, N, N, rows, 0});
+          it.push_back(GemmItem<double, double>{part.p + (slot + z) * r * r, nullptr, r, 0, r, r,
+                                                (int)sg.size() - 1, 1});
+        }
+        slot += ns;
+      }
+    }
+    DevBuf<GemmItem<double, double>> dit;
+    DevBuf<GemmSeg<double>> dsg;
+    DevBuf<SumTask<double>> dst;
+    dit.upload(it);
+    dsg.upload(sg);
+    dst.upload(st);
+    launch_gemm_items<double, double, double>(dit.p, dsg.p, (int)it.size(), r, r, true, 1.0, 0.0,
+                                              s);
+    launch_sum_slots<double>(dst.p, (int)st.size(), (long long)r * r, s);
+    std::vector<double> G(2 * ids.size() * (size_t)r * r);
+    HODLR_CUDA_TRY(cudaMemcpyAsync(G.data(), gram.p, sizeof(double) * G.size(),
+                                   cudaMemcpyDeviceToHost, s));
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    // index of node id in ids
+    std::vector<int> pos(t.nodes.size(), -1);
+    for (size_t q = 0; q < ids.size(); ++q) pos[ids[q]] = (int)q;
+    std::vector<double> scale_u(t.nodes.size(), 1.0), scale_v(t.nodes.size(), 1.0);
+    std::vector<double> v(r), w(r), z(r);
+    for (size_t pi = 0; pi < t.nodes.size(); ++pi) {
+      const Node &P = t.nodes[pi];
+      if (P.is_leaf) continue;
+      const int kids[2] = {P.lchild, P.rchild};
+      for (int side = 0; side < 2; ++side) {
+        const int c = kids[side], sb = kids[1 - side];
+        const double *Gu = G.data() + (2 * (size_t)pos[c] + 0) * r * r;
+        const double *Gv = G.data() + (2 * (size_t)pos[sb] + 1) * r * r;
+        // power iteration on Gu * Gv (similar to a PSD matrix)
+        for (int i = 0; i < r; ++i) v[i] = 1.0 + 0.01 * i;
+        double lam = 0.0;
+        for (int itn = 0; itn < 300; ++itn) {
+          for (int i = 0; i < r; ++i) {
+            double a = 0.0;
+            for (int k = 0; k < r; ++k) a += Gv[i + (size_t)k * r] * v[k];
+            z[i] = a;
+          }
+          double nrm = 0.0;
+          for (int i = 0; i < r; ++i) {
+            double a = 0.0;
+            for (int k = 0; k < r; ++k) a += Gu[i + (size_t)k * r] * z[k];
+            w[i] = a;
+            nrm += a * a;
+          }
+          nrm = std::sqrt(nrm);
+          double vn = 0.0;
+          for (int i = 0; i < r; ++i) vn += v[i] * v[i];
+          lam = nrm / std::sqrt(vn);
+          if (nrm == 0.0) break;
+          for (int i = 0; i < r; ++i) v[i] = w[i] / nrm;
+        }
+        const double norm = std::sqrt(lam);
+        const double f = norm > 0.0 ? std::sqrt(offdiag_norm / norm) : 1.0;
+        scale_u[c] = f;   // U_c and V_sb both take the factor
+        scale_v[sb] = f;
+      }
+    }
+    DevBuf<double> fac;
+    std::vector<double> hf;
+    for (size_t i = 1; i < t.nodes.size(); ++i) { hf.push_back(scale_u[i]); hf.push_back(scale_v[i]); }
+    fac.upload(hf);
+    for (size_t i = 1; i < t.nodes.size(); ++i) {
+      const Node &c = t.nodes[i];
+      launch_scale_cols(S.U.p + c.row_beg + (long long)(c.col_beg - m) * N, N, c.nrow, c.ncol,
+                        fac.p + 2 * (i - 1), s);
+      launch_scale_cols(S.V.p + c.row_beg + (long long)(c.col_beg - m) * N, N, c.nrow, c.vncol,
+                        fac.p + 2 * (i - 1) + 1, s);
+    }
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    S.factored = -1;
+    return 0;
+  });
+}
+
+int hodlr_solve_fused(hodlr_system h, int schur2, int sync, hodlr_stream_t stream) {
+  if (!h) return -1;
+  if (schur2 && 2 * h->sys.r > kMaxNodeS) return HODLR_ERR_UNSUPPORTED;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    h->sys.run_fused64(schur2 ? 1 : 0, s);
+    if (sync) return h->sys.check_info(s);
+    return 0;
+  });
+}
+
+int hodlr_factor(hodlr_system h, int precision, hodlr_stream_t stream) {
+  if (!h) return -1;
+  if (precision != HODLR_PREC_FP64 && precision != HODLR_PREC_MIXED) return -2;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    if (precision == HODLR_PREC_FP64) h->sys.run_fused64(0, s);
+    else h->sys.run_factor32(s);
+    return h->sys.check_info(s);
+  });
+}
+
+int hodlr_solve(hodlr_system h, hodlr_stream_t stream) {
+  if (!h) return -1;
+  System &S = h->sys;
+  if (S.factored < 0) return HODLR_ERR_STATE;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    const size_t nm = (size_t)S.N * S.m;
+    if (S.factored == HODLR_PREC_FP64) {
+      HODLR_CUDA_TRY(cudaMemcpyAsync(S.Y64.p, S.B.p, sizeof(double) * nm, cudaMemcpyDeviceToDevice, s));
+      S.run_apply64(s);
+      HODLR_CUDA_TRY(cudaMemcpyAsync(S.Xsol.p, S.Y64.p, sizeof(double) * nm, cudaMemcpyDeviceToDevice, s));
+    } else {
+      launch_convert2d<double, float>(S.B.p, S.N, S.Y32.p, S.N, S.N, S.m, s);
+      S.run_apply32(s);
+      launch_convert2d<float, double>(S.Y32.p, S.N, S.Xsol.p, S.N, S.N, S.m, s);
+    }
+    return 0;
+  });
+}
+
+int hodlr_solve_refined(hodlr_system h, int precision, double tol, int maxiter, int *iters,
+                        double *relres, hodlr_stream_t stream) {
+  if (!h) return -1;
+  if (precision != HODLR_PREC_FP64 && precision != HODLR_PREC_MIXED) return -2;
+  if (!(tol >= 0.0)) return -3;
+  if (maxiter < 0) return -4;
+  return guarded([&]() -> int {
+    System &S = h->sys;
+    cudaStream_t s = as_stream(stream);
+    const long long N = S.N;
+    const size_t nm = (size_t)N * S.m;
+    if (precision == HODLR_PREC_MIXED) {
+      S.run_factor32(s);
+      launch_convert2d<float, double>(S.X32.p, N, S.Xsol.p, N, N, S.m, s);
+    } else {
+      S.run_fused64(0, s);
+    }
+    int info = S.check_info(s);
+    if (info) return info;
+    int it = 0;
+    double rr = S.relres(s);
+    while (rr > tol && it < maxiter) {
+      if (precision == HODLR_PREC_MIXED) {
+        launch_convert2d<double, float>(S.R64.p, N, S.Y32.p, N, N, S.m, s);
+        S.run_apply32(s);
+        launch_add2d<float>(S.Xsol.p, N, S.Y32.p, N, N, S.m, s);
+      } else {
+        HODLR_CUDA_TRY(cudaMemcpyAsync(S.Y64.p, S.R64.p, sizeof(double) * nm,
+                                       cudaMemcpyDeviceToDevice, s));
+        S.run_apply64(s);
+        launch_add2d<double>(S.Xsol.p, N, S.Y64.p, N, N, S.m, s);
+      }
+      ++it;
+      rr = S.relres(s);
+    }
+    if (iters) *iters = it;
+    if (relres) *relres = rr;
+    return rr <= tol ? 0 : HODLR_ERR_NOCONV;
+  });
+}
+
+int hodlr_matvec(hodlr_system h, const double *x, long long ldx, double *y, long long ldy,
+                 int ncols, hodlr_stream_t stream) {
+  if (!h) return -1;
+  System &S = h->sys;
+  if (!x) return -2;
+  if (ldx < S.N) return -3;
+  if (!y) return -4;
+  if (ldy < S.N) return -5;
+  if (ncols < 0 || ncols > S.m) return -6;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    HODLR_CUDA_TRY(cudaMemsetAsync(S.MVx.p, 0, sizeof(double) * (size_t)S.N * S.m, s));
+    copy2d(S.MVx.p, S.N, x, ldx, S.N, ncols, 0, s);
+    S.run_matvec(S.mv_usr, 1.0, 0.0, s);
+    copy2d(y, ldy, S.R64.p, S.N, S.N, ncols, 0, s);
+    return 0;
+  });
+}
+
+int hodlr_set_profiling(hodlr_system h, int on) {
+  if (!h) return -1;
+  return guarded([&]() -> int {
+    h->sys.prof.reset();
+    h->sys.prof.on = on != 0;
+    return 0;
+  });
+}
+
+int hodlr_phase_times(hodlr_system h, double *ms, long long *launches, int reset) {
+  if (!h) return -1;
+  return guarded([&]() -> int {
+    Profiler &p = h->sys.prof;
+    p.collect();
+    for (int i = 0; i < PH_COUNT; ++i) {
+      if (ms) ms[i] = p.ms[i];
+      if (launches) launches[i] = p.launches[i];
+    }
+    if (reset) p.reset();
+    return 0;
+  });
+}
+
+int hodlr_relres(hodlr_system h, double *relres, hodlr_stream_t stream) {
+  if (!h) return -1;
+  if (!relres) return -2;
+  return guarded([&]() -> int {
+    *relres = h->sys.relres(as_stream(stream));
+    return 0;
+  });
+}
+
+int hodlr_get_solution(hodlr_system h, double *X, long long ldx, int host,
+                       hodlr_stream_t stream) {
+  if (!h) return -1;
+  System &S = h->sys;
+  if (!X) return -2;
+  if (ldx < S.N) return -3;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    HODLR_CUDA_TRY(cudaMemcpy2DAsync(X, sizeof(double) * ldx, S.Xsol.p, sizeof(double) * S.N,
+                                     sizeof(double) * S.N, S.m,
+                                     host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    if (host) HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,554 @@
+// solver.cu -- device-resident HODLR system and its level schedule.
+//
+// The reference launches one Legion task per leaf and per (node, leaf) pair
+// and lets region privileges order them (src/solver/fast_solver.cc:136-255).
+// Here the same dependence structure is a fixed schedule on one stream:
+//   1. every leaf at once: getrf + getrs (solver_tasks.cc:424-450);
+//   2. for each depth d from the deepest internal level up to the root, every
+//      internal node of depth d at once:
+//        reduce  V_c^T [d_c | u_c] for both children (gemm.cc:208-229, as
+//                split-K partial sums, summed in a fixed order by the node
+//                kernel instead of REDOP_ADD atomics),
+//        node    capacitance LU and eta (solver_tasks.cc:139-305),
+//        bcast   d_c -= u_c eta (gemm.cc:232-284).
+// Nodes of equal depth touch disjoint rows, so batching them does not change
+// any operation's inputs; the leaf solves have no inputs from other tasks.
+// All launch descriptors are built once per system and live on the device,
+// so a solve is a fixed sequence of launches (capturable in a CUDA graph).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "gemm_simt.cuh"
+#include "leaf.cuh"
+#include "node.cuh"
+#include "solver.h"
+
+namespace hodlr {
+
+namespace {
+
+template <typename T, typename TE>
+struct PathSpec {
+  T *X = nullptr;           // d columns (and the U columns on factor paths)
+  long long ldx = 0;
+  const T *Usrc = nullptr;  // transformed U columns (== X on factor paths)
+  long long ldu = 0;
+  T *D = nullptr;           // leaf LU factors
+  long long ldd = 0;
+  int *ipiv = nullptr, *perm = nullptr;
+  const T *V = nullptr;
+  long long ldv = 0;
+  T *part = nullptr;
+  TE *eta = nullptr;
+  NodeStore *ns = nullptr;
+  bool factor = false;
+  int red_chunk = 512, bc_chunk = 512;
+};
+
+// Partial-sum and eta workspace (elements) a path needs at its largest level.
+void path_need(const Tree &t, bool factor, int chunk, size_t &part, size_t &eta) {
+  part = 0;
+  eta = 0;
+  for (int d = t.max_depth - 1; d >= 0; --d) {
+    size_t p = 0, e = 0;
+    for (int id : t.internal_at_depth[d]) {
+      const Node &P = t.nodes[id];
+      const Node &c0 = t.nodes[P.lchild], &c1 = t.nodes[P.rchild];
+      const int cw = factor ? c0.col_beg : t.nrhs;
+      for (const Node *c : {&c0, &c1}) {
+        const int NW = factor ? c->col_beg + c->ncol : t.nrhs;
+        p += (size_t)cdiv(c->nrow, chunk) * c->vncol * NW;
+      }
+      e += (size_t)(c0.ncol + c1.ncol) * cw;
+    }
+    part = std::max(part, p);
+    eta = std::max(eta, e);
+  }
+}
+
+template <typename T, typename TE>
+void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan, int form) {
+  plan.levels.clear();
+  plan.factor = sp.factor;
+  const int m = t.nrhs;
+  std::vector<LeafTask<T>> lt;
+  plan.max_n = plan.max_nrhs = 0;
+  for (size_t q = 0; q < t.leaves.size(); ++q) {
+    const Node &n = t.nodes[t.leaves[q]];
+    LeafTask<T> k{};
+    k.D = sp.D + n.row_beg;
+    k.ldd = sp.ldd;
+    k.X = sp.X + n.row_beg;
+    k.ldx = sp.ldx;
+    k.ipiv = sp.ipiv + n.row_beg;
+    k.perm = sp.perm + n.row_beg;
+    k.n = n.nrow;
+    k.nrhs = sp.factor ? n.col_beg + n.ncol : m;
+    k.info_slot = (int)q;
+    plan.max_n = std::max(plan.max_n, k.n);
+    plan.max_nrhs = std::max(plan.max_nrhs, k.nrhs);
+    lt.push_back(k);
+  }
+  plan.nleaf = (int)lt.size();
+  plan.leaf_tasks.upload(lt);
+  const int nleaf = (int)t.leaves.size();
+
+  for (int d = t.max_depth - 1; d >= 0; --d) {
+    const auto &ids = t.internal_at_depth[d];
+    if (ids.empty()) continue;
+    auto L = std::make_unique<LevelPlan<T, TE>>();
+    std::vector<GemmItem<T, T>> ri, bi;
+    std::vector<GemmSeg<T>> rs, bs;
+    std::vector<NodeTask<T, TE>> nt;
+    size_t poff = 0, eoff = 0;
+    for (int p : ids) {
+      const Node &P = t.nodes[p];
+      const Node &c0 = t.nodes[P.lchild], &c1 = t.nodes[P.rchild];
+      const int cw = sp.factor ? c0.col_beg : m;
+      NodeTask<T, TE> k{};
+      for (int side = 0; side < 2; ++side) {
+        const Node &c = side ? c1 : c0;
+        const int NW = sp.factor ? c.col_beg + c.ncol : m;
+        const int M = c.vncol;
+        const int nslots = cdiv(c.nrow, sp.red_chunk);
+        T *slot0 = sp.part + poff;
+        for (int q = 0; q < nslots; ++q) {
+          const int rb = c.row_beg + q * sp.red_chunk;
+          const int rows = std::min(sp.red_chunk, c.row_beg + c.nrow - rb);
+          GemmSeg<T> sg{};
+          sg.A = sp.V + rb + (long long)(c.col_beg - m) * sp.ldv;
+          sg.B = sp.X + rb;
+          sg.lda = sp.ldv;
+          sg.ldb = sp.ldx;
+          sg.K = rows;
+          GemmItem<T, T> it{};
+          it.C = slot0 + (size_t)q * M * NW;
+          it.Cin = nullptr;
+          it.ldc = M;
+          it.M = M;
+          it.N = NW;
+          it.seg_begin = (int)rs.size();
+          it.seg_count = 1;
+          rs.push_back(sg);
+          ri.push_back(it);
+          L->red_max_m = std::max(L->red_max_m, M);
+          L->red_max_n = std::max(L->red_max_n, NW);
+        }
+        poff += (size_t)nslots * M * NW;
+        if (side == 0) {
+          k.W0d = slot0; k.W0u = slot0 + (size_t)M * (NW - c.ncol);
+          k.w0_stride = (long long)M * NW; k.ldw0d = k.ldw0u = M; k.np0 = nslots;
+        } else {
+          k.W1d = slot0; k.W1u = slot0 + (size_t)M * (NW - c.ncol);
+          k.w1_stride = (long long)M * NW; k.ldw1d = k.ldw1u = M; k.np1 = nslots;
+        }
+      }
+      k.r0 = c0.ncol;
+      k.r1 = c1.ncol;
+      k.c = cw;
+      k.eta0 = sp.eta + eoff;
+      k.ld_eta0 = k.r0;
+      eoff += (size_t)k.r0 * cw;
+      k.eta1 = sp.eta + eoff;
+      k.ld_eta1 = k.r1;
+      eoff += (size_t)k.r1 * cw;
+      k.S_lu = sp.ns->S_lu.p + (size_t)p * sp.ns->s_slot;
+      k.S_piv = sp.ns->S_piv.p + (size_t)p * sp.ns->s_max;
+      k.VTu0 = sp.ns->VTu0.p + (size_t)p * sp.ns->rr;
+      k.VTu1 = sp.ns->VTu1.p + (size_t)p * sp.ns->rr;
+      k.info_slot = nleaf + p;
+      nt.push_back(k);
+      const int s = form == 0 ? k.r0 : k.r0 + k.r1;
+      L->max_s = std::max(L->max_s, s);
+      L->max_rs = std::max(L->max_rs, k.r0 + k.r1);
+      L->max_c = std::max(L->max_c, cw);
+      // broadcast d_c -= u_c eta into both children
+      for (int side = 0; side < 2; ++side) {
+        const Node &c = side ? c1 : c0;
+        const TE *eta = side ? k.eta1 : k.eta0;
+        if (cw == 0) continue;
+        for (int rb = c.row_beg; rb < c.row_beg + c.nrow; rb += sp.bc_chunk) {
+          const int rows = std::min(sp.bc_chunk, c.row_beg + c.nrow - rb);
+          GemmSeg<T> sg{};
+          sg.A = sp.Usrc + rb + (long long)c.col_beg * sp.ldu;
+          sg.B = reinterpret_cast<const T *>(eta);
+          sg.lda = sp.ldu;
+          sg.ldb = c.ncol;
+          sg.K = c.ncol;
+          GemmItem<T, T> it{};
+          it.C = sp.X + rb;
+          it.Cin = sp.X + rb;
+          it.ldc = it.ldcin = sp.ldx;
+          it.M = rows;
+          it.N = cw;
+          it.seg_begin = (int)bs.size();
+          it.seg_count = 1;
+          bs.push_back(sg);
+          bi.push_back(it);
+          L->bc_max_m = std::max(L->bc_max_m, rows);
+          L->bc_max_n = std::max(L->bc_max_n, cw);
+        }
+      }
+    }
+    L->red_items.upload(ri);
+    L->red_segs.upload(rs);
+    L->n_red = (int)ri.size();
+    L->node_tasks.upload(nt);
+    L->n_nodes = (int)nt.size();
+    L->bc_items.upload(bi);
+    L->bc_segs.upload(bs);
+    L->n_bc = (int)bi.size();
+    plan.levels.push_back(std::move(L));
+  }
+  plan.built = true;
+}
+
+// RAII phase marker: records a CUDA event pair when profiling is on.
+struct PhaseScope {
+  Profiler &p;
+  int ph;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr;
+  PhaseScope(Profiler &p_, int ph_, cudaStream_t s_) : p(p_), ph(ph_), s(s_) {
+    if (p.on) p.begin(ph, s, a);
+  }
+  ~PhaseScope() {
+    if (p.on) p.end(ph, s, a);
+  }
+};
+
+template <typename T, typename TE>
+void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cudaStream_t s) {
+  LeafTask<T> none{};
+  if (plan.factor) {
+    PhaseScope ps(pf, PH_GETRF, s);
+    launch_getrf<T>(plan.leaf_tasks.p, none, plan.nleaf, plan.max_n, info, s);
+  }
+  {
+    PhaseScope ps(pf, PH_GETRS, s);
+    launch_getrs<T>(plan.leaf_tasks.p, none, plan.nleaf, plan.max_n, plan.max_nrhs, s);
+  }
+  for (const auto &Lp : plan.levels) {
+    const LevelPlan<T, TE> &L = *Lp;
+    {
+      PhaseScope ps(pf, PH_REDUCE, s);
+      launch_gemm_items<T, T, T>(L.red_items.p, L.red_segs.p, L.n_red, L.red_max_m,
+                                 L.red_max_n, true, T(1), T(0), s);
+    }
+    if (plan.factor) {
+      PhaseScope ps(pf, PH_NODE_FACTOR, s);
+      launch_node_factor<T, TE>(L.node_tasks.p, L.n_nodes, L.max_s, form, info, s);
+    }
+    {
+      PhaseScope ps(pf, PH_NODE_APPLY, s);
+      launch_node_apply<T, TE>(L.node_tasks.p, L.n_nodes, L.max_s, L.max_rs, L.max_c, form, s);
+    }
+    {
+      PhaseScope ps(pf, PH_BCAST, s);
+      launch_gemm_items<T, T, T>(L.bc_items.p, L.bc_segs.p, L.n_bc, L.bc_max_m, L.bc_max_n,
+                                 false, T(-1), T(1), s);
+    }
+  }
+}
+
+void alloc_node_store(NodeStore &ns, const Tree &t) {
+  const int r = t.rank;
+  ns.s_max = (2 * r <= kMaxNodeS) ? 2 * r : r;
+  ns.s_slot = ns.s_max * ns.s_max;
+  ns.rr = r * r;
+  const size_t nn = t.nodes.size();
+  ns.S_lu.ensure(nn * ns.s_slot);
+  ns.S_piv.ensure(nn * ns.s_max);
+  ns.VTu0.ensure(nn * ns.rr);
+  ns.VTu1.ensure(nn * ns.rr);
+}
+
+void build_matvec(System &S, const double *x, MatvecPlan &mv) {
+  const Tree &t = S.tree;
+  const int m = S.m;
+  const long long N = S.N;
+  const int chunk = 2048;
+  std::vector<GemmItem<double, double>> ri, ai;
+  std::vector<GemmSeg<double>> rs, as;
+  std::vector<SumTask<double>> su;
+  std::vector<size_t> toff(t.nodes.size(), 0);
+  size_t poff = 0, tsz = 0;
+  for (size_t i = 1; i < t.nodes.size(); ++i) {
+    const Node &c = t.nodes[i];
+    toff[i] = tsz;
+    tsz += (size_t)c.vncol * m;
+  }
+  size_t pneed = 0;
+  for (size_t i = 1; i < t.nodes.size(); ++i)
+    pneed += (size_t)cdiv(t.nodes[i].nrow, chunk) * t.nodes[i].vncol * m;
+  S.tbuf.ensure(std::max<size_t>(tsz, 1));
+  S.mvpart.ensure(std::max<size_t>(pneed, 1));
+  mv.red_max_m = mv.red_max_n = 0;
+  for (size_t i = 1; i < t.nodes.size(); ++i) {
+    const Node &c = t.nodes[i];
+    const int M = c.vncol;
+    const int nslots = cdiv(c.nrow, chunk);
+    double *slot0 = S.mvpart.p + poff;
+    for (int q = 0; q < nslots; ++q) {
+      const int rb = c.row_beg + q * chunk;
+      const int rows = std::min(chunk, c.row_beg + c.nrow - rb);
+      GemmSeg<double> sg{};
+      sg.A = S.V.p + rb + (long long)(c.col_beg - m) * N;
+      sg.B = x + rb;
+      sg.lda = N;
+      sg.ldb = N;
+      sg.K = rows;
+      GemmItem<double, double> it{};
+      it.C = slot0 + (size_t)q * M * m;
+      it.ldc = M;
+      it.M = M;
+      it.N = m;
+      it.seg_begin = (int)rs.size();
+      it.seg_count = 1;
+      rs.push_back(sg);
+      ri.push_back(it);
+      mv.red_max_m = std::max(mv.red_max_m, M);
+      mv.red_max_n = std::max(mv.red_max_n, m);
+    }
+    SumTask<double> st{};
+    st.dst = S.tbuf.p + toff[i];
+    st.src = slot0;
+    st.len = (long long)M * m;
+    st.stride = (long long)M * m;
+    st.nslots = nslots;
+    su.push_back(st);
+    mv.sum_max_len = std::max(mv.sum_max_len, st.len);
+    poff += (size_t)nslots * M * m;
+  }
+  mv.ap_max_m = mv.ap_max_n = 0;
+  for (int leaf : t.leaves) {
+    const Node &n = t.nodes[leaf];
+    GemmItem<double, double> it{};
+    it.C = S.R64.p + n.row_beg;
+    it.Cin = S.B.p + n.row_beg;
+    it.ldc = N;
+    it.ldcin = N;
+    it.M = n.nrow;
+    it.N = m;
+    it.seg_begin = (int)as.size();
+    GemmSeg<double> sd{};
+    sd.A = S.D.p + n.row_beg;
+    sd.lda = N;
+    sd.B = x + n.row_beg;
+    sd.ldb = N;
+    sd.K = n.nrow;
+    as.push_back(sd);
+    for (int a = leaf; a > 0; a = t.nodes[a].parent) {
+      const Node &an = t.nodes[a];
+      const Node &pa = t.nodes[an.parent];
+      const int sib = (pa.lchild == a) ? pa.rchild : pa.lchild;
+      GemmSeg<double> su_{};
+      su_.A = S.U.p + n.row_beg + (long long)(an.col_beg - m) * N;
+      su_.lda = N;
+      su_.B = S.tbuf.p + toff[sib];
+      su_.ldb = an.ncol;
+      su_.K = an.ncol;
+      as.push_back(su_);
+    }
+    it.seg_count = (int)as.size() - it.seg_begin;
+    ai.push_back(it);
+    mv.ap_max_m = std::max(mv.ap_max_m, n.nrow);
+    mv.ap_max_n = std::max(mv.ap_max_n, m);
+  }
+  mv.red_items.upload(ri);
+  mv.red_segs.upload(rs);
+  mv.n_red = (int)ri.size();
+  mv.sums.upload(su);
+  mv.n_sums = (int)su.size();
+  mv.ap_items.upload(ai);
+  mv.ap_segs.upload(as);
+  mv.n_ap = (int)ai.size();
+  mv.built = true;
+}
+
+}  // namespace
+
+void Profiler::begin(int ph, cudaStream_t s, cudaEvent_t &a) {
+  HODLR_CUDA_TRY(cudaEventCreate(&a));
+  HODLR_CUDA_TRY(cudaEventRecord(a, s));
+  (void)ph;
+}
+void Profiler::end(int ph, cudaStream_t s, cudaEvent_t a) {
+  cudaEvent_t b;
+  HODLR_CUDA_TRY(cudaEventCreate(&b));
+  HODLR_CUDA_TRY(cudaEventRecord(b, s));
+  recs.push_back({ph, a, b});
+}
+void Profiler::collect() {
+  for (auto &r : recs) {
+    HODLR_CUDA_TRY(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    HODLR_CUDA_TRY(cudaEventElapsedTime(&t, r.a, r.b));
+    ms[r.phase] += t;
+    launches[r.phase] += 1;
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  recs.clear();
+}
+void Profiler::reset() {
+  collect();
+  for (int i = 0; i < PH_COUNT; ++i) { ms[i] = 0; launches[i] = 0; }
+}
+
+int System::init(int N_, int nrhs, int rank, int threshold) {
+  int rc = build_tree(N_, nrhs, rank, threshold, tree);
+  if (rc) return rc;
+  if (2 * rank > kMaxNodeS && rank > kMaxNodeS) return -3;
+  N = N_;
+  m = nrhs;
+  r = rank;
+  C = tree.ncols;
+  vc = tree.vcols();
+  nmax = tree.max_leaf;
+  const size_t n = (size_t)N;
+  D.ensure(n * nmax);
+  U.ensure(n * std::max(vc, 1));
+  V.ensure(n * std::max(vc, 1));
+  B.ensure(n * m);
+  Xsol.ensure(n * m);
+  R64.ensure(n * m);
+  MVx.ensure(n * m);
+  relres_dev.ensure(m);
+  n_info = (int)(tree.leaves.size() + tree.nodes.size());
+  info.ensure(n_info);
+  HODLR_CUDA_TRY(cudaMemset(info.p, 0, sizeof(int) * n_info));
+  HODLR_CUDA_TRY(cudaMemset(D.p, 0, sizeof(double) * n * nmax));
+  HODLR_CUDA_TRY(cudaMemset(U.p, 0, sizeof(double) * n * std::max(vc, 1)));
+  HODLR_CUDA_TRY(cudaMemset(V.p, 0, sizeof(double) * n * std::max(vc, 1)));
+  HODLR_CUDA_TRY(cudaMemset(B.p, 0, sizeof(double) * n * m));
+  HODLR_CUDA_TRY(cudaMemset(Xsol.p, 0, sizeof(double) * n * m));
+  build_matvec(*this, Xsol.p, mv_sol);
+  build_matvec(*this, MVx.p, mv_usr);
+  return 0;
+}
+
+void System::ensure_fp64() {
+  if (fused64[0].built) return;
+  const size_t n = (size_t)N;
+  X64.ensure(n * C);
+  DLU64.ensure(n * nmax);
+  Y64.ensure(n * m);
+  ipiv64.ensure(n);
+  perm64.ensure(n);
+  alloc_node_store(ns64, tree);
+  size_t pf, ef, pa, ea;
+  path_need(tree, true, red_chunk, pf, ef);
+  path_need(tree, false, red_chunk, pa, ea);
+  part64.ensure(std::max<size_t>(std::max(pf, pa), 1));
+  eta64.ensure(std::max<size_t>(std::max(ef, ea), 1));
+  for (int form = 0; form < 2; ++form) {
+    if (form == 1 && ns64.s_max < 2 * r) continue;
+    PathSpec<double, double> f;
+    f.X = X64.p; f.ldx = N; f.Usrc = X64.p; f.ldu = N;
+    f.D = DLU64.p; f.ldd = N; f.ipiv = ipiv64.p; f.perm = perm64.p;
+    f.V = V.p; f.ldv = N; f.part = part64.p; f.eta = eta64.p; f.ns = &ns64;
+    f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk;
+    build_path(tree, f, fused64[form], form);
+    PathSpec<double, double> a = f;
+    a.X = Y64.p; a.factor = false;
+    build_path(tree, a, apply64[form], form);
+  }
+}
+
+void System::ensure_mixed() {
+  if (fused32.built) return;
+  const size_t n = (size_t)N;
+  X32.ensure(n * C);
+  D32.ensure(n * nmax);
+  V32.ensure(n * std::max(vc, 1));
+  Y32.ensure(n * m);
+  ipiv32.ensure(n);
+  perm32.ensure(n);
+  alloc_node_store(ns32, tree);
+  size_t pf, ef, pa, ea;
+  path_need(tree, true, red_chunk, pf, ef);
+  path_need(tree, false, red_chunk, pa, ea);
+  part32.ensure(std::max<size_t>(std::max(pf, pa), 1));
+  eta32.ensure(std::max<size_t>(std::max(ef, ea), 1));
+  PathSpec<float, float> f;
+  f.X = X32.p; f.ldx = N; f.Usrc = X32.p; f.ldu = N;
+  f.D = D32.p; f.ldd = N; f.ipiv = ipiv32.p; f.perm = perm32.p;
+  f.V = V32.p; f.ldv = N; f.part = part32.p; f.eta = eta32.p; f.ns = &ns32;
+  f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk;
+  build_path(tree, f, fused32, 0);
+  PathSpec<float, float> a = f;
+  a.X = Y32.p; a.factor = false;
+  build_path(tree, a, apply32, 0);
+}
+
+void System::run_fused64(int form, cudaStream_t s) {
+  ensure_fp64();
+  const size_t n = (size_t)N;
+  HODLR_CUDA_TRY(cudaMemcpyAsync(DLU64.p, D.p, sizeof(double) * n * nmax, cudaMemcpyDeviceToDevice, s));
+  HODLR_CUDA_TRY(cudaMemcpyAsync(X64.p, B.p, sizeof(double) * n * m, cudaMemcpyDeviceToDevice, s));
+  if (vc > 0)
+    HODLR_CUDA_TRY(cudaMemcpyAsync(X64.p + n * m, U.p, sizeof(double) * n * vc,
+                                   cudaMemcpyDeviceToDevice, s));
+  run_path(prof, fused64[form], form, info.p, s);
+  HODLR_CUDA_TRY(cudaMemcpyAsync(Xsol.p, X64.p, sizeof(double) * n * m, cudaMemcpyDeviceToDevice, s));
+  factored = HODLR_PREC_FP64;
+  factored_form = form;
+}
+
+void System::run_apply64(cudaStream_t s) {
+  run_path(prof, apply64[factored_form], factored_form, nullptr, s);
+}
+
+void System::run_factor32(cudaStream_t s) {
+  ensure_mixed();
+  const long long n = N;
+  {
+    PhaseScope ps(prof, PH_CONVERT, s);
+    launch_convert2d<double, float>(D.p, n, D32.p, n, n, nmax, s);
+    launch_convert2d<double, float>(B.p, n, X32.p, n, n, m, s);
+    if (vc > 0) {
+      launch_convert2d<double, float>(U.p, n, X32.p + (size_t)n * m, n, n, vc, s);
+      launch_convert2d<double, float>(V.p, n, V32.p, n, n, vc, s);
+    }
+  }
+  run_path(prof, fused32, 0, info.p, s);
+  factored = HODLR_PREC_MIXED;
+  factored_form = 0;
+}
+
+void System::run_apply32(cudaStream_t s) { run_path(prof, apply32, 0, nullptr, s); }
+
+void System::run_matvec(const MatvecPlan &p, double alpha, double beta, cudaStream_t s) {
+  PhaseScope ps(prof, PH_MATVEC, s);
+  launch_gemm_items<double, double, double>(p.red_items.p, p.red_segs.p, p.n_red, p.red_max_m,
+                                            p.red_max_n, true, 1.0, 0.0, s);
+  launch_sum_slots<double>(p.sums.p, p.n_sums, p.sum_max_len, s);
+  launch_gemm_items<double, double, double>(p.ap_items.p, p.ap_segs.p, p.n_ap, p.ap_max_m,
+                                            p.ap_max_n, false, alpha, beta, s);
+}
+
+int System::check_info(cudaStream_t s) {
+  std::vector<int> h(n_info);
+  HODLR_CUDA_TRY(cudaMemcpyAsync(h.data(), info.p, sizeof(int) * n_info, cudaMemcpyDeviceToHost, s));
+  HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+  const int nleaf = (int)tree.leaves.size();
+  for (int i = 0; i < n_info; ++i)
+    if (h[i] != 0) return i < nleaf ? h[i] : 100000 + h[i];
+  return 0;
+}
+
+double System::relres(cudaStream_t s) {
+  run_matvec(mv_sol, -1.0, 1.0, s);
+  launch_colratio(R64.p, N, B.p, N, N, m, relres_dev.p, s);
+  std::vector<double> h(m);
+  HODLR_CUDA_TRY(cudaMemcpyAsync(h.data(), relres_dev.p, sizeof(double) * m,
+                                 cudaMemcpyDeviceToHost, s));
+  HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+  double mx = 0.0;
+  for (double v : h) mx = std::max(mx, std::isnan(v) ? INFINITY : v);
+  return mx;
+}
+
+}  // namespace hodlr

@@ -1,0 +1,149 @@
+// solver.h -- one HODLR system on the device and the level schedule that
+// replaces fastSolver's Legion task launches (FastSolver::bfs_solve,
+// src/solver/fast_solver.cc:56-72, 136-255).
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "htree.h"
+#include "util.cuh"
+
+namespace hodlr {
+
+// Grow-only device buffer.
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void ensure(size_t count) {
+    if (count <= n && p) return;
+    release();
+    size_t bytes = sizeof(T) * (count ? count : 1);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();
+      throw CudaError{e};
+    }
+    n = count;
+  }
+  void upload(const std::vector<T> &v) {
+    ensure(v.size());
+    if (!v.empty()) HODLR_CUDA_TRY(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  }
+};
+
+// Per-node factorization data kept for solves with the same factors.
+struct NodeStore {
+  DevBuf<double> S_lu;   // per node: s_slot doubles
+  DevBuf<int> S_piv;     // per node: s_max ints
+  DevBuf<double> VTu0;   // per node: r*r
+  DevBuf<double> VTu1;
+  int s_slot = 0, s_max = 0, rr = 0;
+};
+
+template <typename T, typename TE>
+struct LevelPlan {
+  DevBuf<GemmItem<T, T>> red_items;
+  DevBuf<GemmSeg<T>> red_segs;
+  int n_red = 0, red_max_m = 0, red_max_n = 0;
+  DevBuf<NodeTask<T, TE>> node_tasks;
+  int n_nodes = 0, max_s = 0, max_rs = 0, max_c = 0;
+  DevBuf<GemmItem<T, T>> bc_items;
+  DevBuf<GemmSeg<T>> bc_segs;
+  int n_bc = 0, bc_max_m = 0, bc_max_n = 0;
+};
+
+template <typename T, typename TE>
+struct PathPlan {
+  bool built = false;
+  bool factor = false;  // getrf + node factor (fused) vs getrs + node apply only
+  DevBuf<LeafTask<T>> leaf_tasks;
+  int nleaf = 0, max_n = 0, max_nrhs = 0;
+  std::vector<std::unique_ptr<LevelPlan<T, TE>>> levels;  // deepest first
+};
+
+// Matvec plan: y = beta b + alpha (D x + sum_c U_c V_sib^T x_sib).
+struct MatvecPlan {
+  bool built = false;
+  DevBuf<GemmItem<double, double>> red_items;
+  DevBuf<GemmSeg<double>> red_segs;
+  int n_red = 0, red_max_m = 0, red_max_n = 0;
+  DevBuf<SumTask<double>> sums;
+  int n_sums = 0;
+  long long sum_max_len = 0;
+  DevBuf<GemmItem<double, double>> ap_items;
+  DevBuf<GemmSeg<double>> ap_segs;
+  int n_ap = 0, ap_max_m = 0, ap_max_n = 0;
+};
+
+// Optional per-phase timing (CUDA events around each launch group).
+enum Phase {
+  PH_GETRF = 0, PH_GETRS, PH_REDUCE, PH_NODE_FACTOR, PH_NODE_APPLY, PH_BCAST, PH_MATVEC,
+  PH_CONVERT, PH_COUNT
+};
+struct Profiler {
+  bool on = false;
+  struct Rec { int phase; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  double ms[PH_COUNT] = {0};
+  long long launches[PH_COUNT] = {0};
+  void begin(int ph, cudaStream_t s, cudaEvent_t &a);
+  void end(int ph, cudaStream_t s, cudaEvent_t a);
+  void collect();  // sync + accumulate + free events
+  void reset();
+};
+
+struct System {
+  Tree tree;
+  int N = 0, m = 0, r = 0, C = 0, vc = 0, nmax = 0;
+  // originals (FP64)
+  DevBuf<double> D, U, V, B, Xsol;
+  // FP64 path
+  DevBuf<double> X64, DLU64, Y64;
+  DevBuf<int> ipiv64, perm64;
+  // mixed path
+  DevBuf<float> X32, D32, V32, Y32;
+  DevBuf<int> ipiv32, perm32;
+  DevBuf<double> R64, MVx, relres_dev;
+  // workspaces
+  DevBuf<double> part64, eta64, tbuf, mvpart;
+  DevBuf<float> part32, eta32;
+  DevBuf<int> info;
+  NodeStore ns64, ns32;
+  PathPlan<double, double> fused64[2];  // [form]
+  PathPlan<double, double> apply64[2];
+  PathPlan<float, float> fused32, apply32;
+  MatvecPlan mv_sol, mv_usr;
+  int factored = -1;  // HODLR_PREC_* of the current factorization, -1 none
+  int factored_form = 0;
+  int red_chunk = 512;
+  int bc_chunk = 512;
+  int n_info = 0;
+  Profiler prof;
+
+  int init(int N_, int nrhs, int rank, int threshold);
+  void ensure_fp64();
+  void ensure_mixed();
+
+  void run_fused64(int form, cudaStream_t s);     // X64 = [B|U], DLU64 = D, walk
+  void run_apply64(cudaStream_t s);               // Y64 <- A^{-1} Y64 with fused64 factors
+  void run_factor32(cudaStream_t s);              // X32 = f32([B|U]), D32 = f32(D), walk
+  void run_apply32(cudaStream_t s);               // Y32 <- A^{-1} Y32
+  void run_matvec(const MatvecPlan &p, double alpha, double beta, cudaStream_t s);
+  int check_info(cudaStream_t s);                 // sync + first nonzero INFO
+  double relres(cudaStream_t s);                  // of Xsol against B (sync)
+};
+
+}  // namespace hodlr

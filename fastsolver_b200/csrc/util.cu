@@ -1,0 +1,271 @@
+// util.cu -- element-wise kernels and device-side generators.
+#include "common.cuh"
+#include "util.cuh"
+
+namespace hodlr {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int grid_for(long long n) {
+  long long b = (n + kThreads - 1) / kThreads;
+  if (b > 148LL * 64) b = 148LL * 64;
+  return (int)(b > 0 ? b : 1);
+}
+
+template <typename TS, typename TD>
+__global__ void convert2d_kernel(const TS *__restrict__ src, long long lds, TD *__restrict__ dst,
+                                 long long ldd, long long rows, long long cols) {
+  const long long total = rows * cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e % rows, j = e / rows;
+    dst[i + j * ldd] = TD(src[i + j * lds]);
+  }
+}
+
+template <typename TS>
+__global__ void add2d_kernel(double *__restrict__ x, long long ldx, const TS *__restrict__ y,
+                             long long ldy, long long rows, long long cols) {
+  const long long total = rows * cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e % rows, j = e / rows;
+    x[i + j * ldx] += double(y[i + j * ldy]);
+  }
+}
+
+// out[c] = sqrt(sum_i r(i,c)^2) / sqrt(sum_i b(i,c)^2), one CTA per column.
+__global__ void colratio_kernel(const double *__restrict__ r, long long ldr,
+                                const double *__restrict__ b, long long ldb, long long rows,
+                                double *__restrict__ out) {
+  __shared__ double sr[32], sb[32];
+  const int c = blockIdx.x;
+  double ar = 0.0, ab = 0.0;
+  for (long long i = threadIdx.x; i < rows; i += blockDim.x) {
+    const double x = r[i + c * ldr], y = b[i + c * ldb];
+    ar += x * x;
+    ab += y * y;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    ar += __shfl_down_sync(0xffffffffu, ar, off);
+    ab += __shfl_down_sync(0xffffffffu, ab, off);
+  }
+  if ((threadIdx.x & 31) == 0) { sr[threadIdx.x >> 5] = ar; sb[threadIdx.x >> 5] = ab; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tr = 0.0, tb = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tr += sr[w]; tb += sb[w]; }
+    out[c] = tb > 0.0 ? sqrt(tr) / sqrt(tb) : sqrt(tr);
+  }
+}
+
+// dst[t][e] = sum_q src[t] + q * stride, fixed order (deterministic)
+template <typename T>
+__global__ void sum_slots_kernel(const SumTask<T> *__restrict__ tasks) {
+  const SumTask<T> tk = tasks[blockIdx.y];
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tk.len;
+       e += (long long)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int q = 0; q < tk.nslots; ++q) acc += double(tk.src[e + q * tk.stride]);
+    tk.dst[e] = T(acc);
+  }
+}
+
+__global__ void scale_cols_kernel(double *__restrict__ a, long long lda, long long rows,
+                                  int cols, const double *__restrict__ s) {
+  const long long total = rows * cols;
+  const double f = *s;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e % rows, j = e / rows;
+    a[i + j * lda] *= f;
+  }
+}
+
+// ----- generators ----------------------------------------------------------
+
+// Reference test matrix: leaf block K = U U^T + diag I, U(i,j) = (g + i + j) % r
+// with g the leaf's first global row (hodlr_matrix.cc:528-567).  Entries are
+// exact integers (plus diag), so the result equals the reference's dgemm.
+__global__ void circulant_k_kernel(const int2 *__restrict__ leaves, int nleaves, double *D,
+                                   long long ldd, int r, double diag) {
+  const int2 lf = leaves[blockIdx.y];  // (row_beg, nrow)
+  const long long n = lf.y;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n * n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e % n, j = e / n;
+    const long long gi = lf.x + i, gj = lf.x + j;
+    double acc = (i == j) ? diag : 0.0;
+    for (int k = 0; k < r; ++k) acc += double((gi + k) % r) * double((gj + k) % r);
+    D[lf.x + i + j * ldd] = acc;
+  }
+}
+
+// U = V = (i + j) % r in global rows, every level block the same
+// (init_matrix_tasks.cc:176-219 with the Hmat/U column layout).
+__global__ void circulant_uv_kernel(double *U, long long ldu, double *V, long long ldv,
+                                    long long N, int vcols, int r) {
+  const long long total = N * vcols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e % N;
+    const int j = (int)(e / N);
+    const double v = double((i + (j % r)) % r);
+    U[i + j * ldu] = v;
+    V[i + j * ldv] = v;
+  }
+}
+
+// drand48_r stream, reseeded per leaf, row-major fill (init_matrix_tasks.cc:
+// 66-76): x = (seed << 16) | 0x330E; x' = (0x5DEECE66D x + 0xB) mod 2^48.
+__global__ void drand48_kernel(const int2 *__restrict__ leaves, int nleaves, double *B,
+                               long long ldb, int m, long seed) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nleaves) return;
+  const int2 lf = leaves[q];
+  unsigned long long x = ((unsigned long long)(unsigned int)seed << 16) | 0x330Eull;
+  const unsigned long long a = 0x5DEECE66Dull, c = 0xBull, mask = (1ull << 48) - 1;
+  for (int i = 0; i < lf.y; ++i)
+    for (int j = 0; j < m; ++j) {
+      x = (a * x + c) & mask;
+      B[lf.x + i + (long long)j * ldb] = ldexp((double)x, -48);
+    }
+}
+
+// Philox4x32-10 (Salmon et al., "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11): 10 rounds of the 4x32 bijection with the published multipliers
+// and Weyl key increments.
+__device__ inline uint4 philox4x32_10(uint4 ctr, uint2 key) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(M0, ctr.x), lo0 = M0 * ctr.x;
+    const uint32_t hi1 = __umulhi(M1, ctr.z), lo1 = M1 * ctr.z;
+    ctr = make_uint4(hi1 ^ ctr.y ^ key.x, lo1, hi0 ^ ctr.w ^ key.y, lo0);
+    key.x += W0;
+    key.y += W1;
+  }
+  return ctr;
+}
+
+__device__ inline double u53(uint32_t hi, uint32_t lo) {
+  // (0, 1]: 53 random bits, never zero (safe for log)
+  const unsigned long long v = ((unsigned long long)hi << 21) ^ (unsigned long long)lo;
+  return (double)((v & ((1ull << 53) - 1)) + 1) * 0x1.0p-53;
+}
+
+// a(i, j) = scale * N(0,1) [+ add on the diagonal i == j - diag_off]
+// for i < rows, j < cols; `stream_id` separates independent fills.
+__global__ void gauss_fill_kernel(double *a, long long lda, long long rows, long long cols,
+                                  unsigned long long seed, unsigned int stream_id, double scale,
+                                  double diag_add, long long diag_row0) {
+  const long long total = rows * cols;
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  for (long long e2 = blockIdx.x * (long long)blockDim.x + threadIdx.x; 2 * e2 < total;
+       e2 += (long long)gridDim.x * blockDim.x) {
+    const uint4 ctr = make_uint4((uint32_t)e2, (uint32_t)(e2 >> 32), stream_id, 0x5eedu);
+    const uint4 rv = philox4x32_10(ctr, key);
+    const double u1 = u53(rv.x, rv.y), u2 = u53(rv.z, rv.w);
+    const double rad = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    const double g[2] = {rad * cs, rad * sn};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long long e = 2 * e2 + h;
+      if (e >= total) break;
+      const long long i = e % rows, j = e / rows;
+      double v = scale * g[h];
+      if (i - diag_row0 == j) v += diag_add;
+      a[i + j * lda] = v;
+    }
+  }
+}
+
+}  // namespace
+
+template <typename TS, typename TD>
+void launch_convert2d(const TS *src, long long lds, TD *dst, long long ldd, long long rows,
+                      long long cols, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  convert2d_kernel<TS, TD><<<grid_for(rows * cols), kThreads, 0, s>>>(src, lds, dst, ldd, rows,
+                                                                       cols);
+  HODLR_LAUNCH_CHECK();
+}
+template void launch_convert2d<double, float>(const double *, long long, float *, long long,
+                                              long long, long long, cudaStream_t);
+template void launch_convert2d<float, double>(const float *, long long, double *, long long,
+                                              long long, long long, cudaStream_t);
+template void launch_convert2d<double, double>(const double *, long long, double *, long long,
+                                               long long, long long, cudaStream_t);
+
+template <typename TS>
+void launch_add2d(double *x, long long ldx, const TS *y, long long ldy, long long rows,
+                  long long cols, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  add2d_kernel<TS><<<grid_for(rows * cols), kThreads, 0, s>>>(x, ldx, y, ldy, rows, cols);
+  HODLR_LAUNCH_CHECK();
+}
+template void launch_add2d<float>(double *, long long, const float *, long long, long long,
+                                  long long, cudaStream_t);
+template void launch_add2d<double>(double *, long long, const double *, long long, long long,
+                                   long long, cudaStream_t);
+
+void launch_colratio(const double *r, long long ldr, const double *b, long long ldb,
+                     long long rows, int cols, double *out, cudaStream_t s) {
+  if (cols <= 0) return;
+  colratio_kernel<<<cols, 1024, 0, s>>>(r, ldr, b, ldb, rows, out);
+  HODLR_LAUNCH_CHECK();
+}
+
+template <typename T>
+void launch_sum_slots(const SumTask<T> *tasks, int ntasks, long long max_len, cudaStream_t s) {
+  if (ntasks <= 0 || max_len <= 0) return;
+  dim3 grid((unsigned)std::min<long long>(cdiv<long long>(max_len, kThreads), 4096), ntasks);
+  sum_slots_kernel<T><<<grid, kThreads, 0, s>>>(tasks);
+  HODLR_LAUNCH_CHECK();
+}
+template void launch_sum_slots<double>(const SumTask<double> *, int, long long, cudaStream_t);
+
+void launch_scale_cols(double *a, long long lda, long long rows, int cols, const double *s_dev,
+                       cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  scale_cols_kernel<<<grid_for(rows * cols), kThreads, 0, s>>>(a, lda, rows, cols, s_dev);
+  HODLR_LAUNCH_CHECK();
+}
+
+void launch_circulant_k(const int2 *leaves, int nleaves, int max_leaf, double *D,
+                        long long ldd, int r, double diag, cudaStream_t s) {
+  if (nleaves <= 0) return;
+  dim3 grid(cdiv<long long>((long long)max_leaf * max_leaf, kThreads), nleaves);
+  circulant_k_kernel<<<grid, kThreads, 0, s>>>(leaves, nleaves, D, ldd, r, diag);
+  HODLR_LAUNCH_CHECK();
+}
+
+void launch_circulant_uv(double *U, long long ldu, double *V, long long ldv, long long N,
+                         int vcols, int r, cudaStream_t s) {
+  if (N <= 0 || vcols <= 0) return;
+  circulant_uv_kernel<<<grid_for(N * vcols), kThreads, 0, s>>>(U, ldu, V, ldv, N, vcols, r);
+  HODLR_LAUNCH_CHECK();
+}
+
+void launch_drand48(const int2 *leaves, int nleaves, double *B, long long ldb, int m,
+                    long seed, cudaStream_t s) {
+  if (nleaves <= 0) return;
+  drand48_kernel<<<cdiv(nleaves, 128), 128, 0, s>>>(leaves, nleaves, B, ldb, m, seed);
+  HODLR_LAUNCH_CHECK();
+}
+
+void launch_gauss_fill(double *a, long long lda, long long rows, long long cols,
+                       unsigned long long seed, unsigned int stream_id, double scale,
+                       double diag_add, long long diag_row0, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  gauss_fill_kernel<<<grid_for((rows * cols + 1) / 2), kThreads, 0, s>>>(
+      a, lda, rows, cols, seed, stream_id, scale, diag_add, diag_row0);
+  HODLR_LAUNCH_CHECK();
+}
+
+}  // namespace hodlr

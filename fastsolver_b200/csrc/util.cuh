@@ -1,0 +1,43 @@
+// util.cuh -- element-wise kernels and device generators (util.cu).
+#pragma once
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace hodlr {
+
+// dst[t][0:len) = sum over q < nslots of src[t][q * stride + 0:len)
+template <typename T>
+struct SumTask {
+  T *dst;
+  const T *src;
+  long long len;
+  long long stride;
+  int nslots;
+  int pad;
+};
+
+template <typename TS, typename TD>
+void launch_convert2d(const TS *src, long long lds, TD *dst, long long ldd, long long rows,
+                      long long cols, cudaStream_t s);
+template <typename TS>
+void launch_add2d(double *x, long long ldx, const TS *y, long long ldy, long long rows,
+                  long long cols, cudaStream_t s);
+void launch_colratio(const double *r, long long ldr, const double *b, long long ldb,
+                     long long rows, int cols, double *out, cudaStream_t s);
+template <typename T>
+void launch_sum_slots(const SumTask<T> *tasks, int ntasks, long long max_len, cudaStream_t s);
+void launch_scale_cols(double *a, long long lda, long long rows, int cols, const double *s_dev,
+                       cudaStream_t s);
+
+void launch_circulant_k(const int2 *leaves, int nleaves, int max_leaf, double *D,
+                        long long ldd, int r, double diag, cudaStream_t s);
+void launch_circulant_uv(double *U, long long ldu, double *V, long long ldv, long long N,
+                         int vcols, int r, cudaStream_t s);
+void launch_drand48(const int2 *leaves, int nleaves, double *B, long long ldb, int m,
+                    long seed, cudaStream_t s);
+void launch_gauss_fill(double *a, long long lda, long long rows, long long cols,
+                       unsigned long long seed, unsigned int stream_id, double scale,
+                       double diag_add, long long diag_row0, cudaStream_t s);
+
+}  // namespace hodlr

@@ -1,0 +1,233 @@
+/*
+ * hodlr_gpu.h -- C ABI of the B200 HODLR direct solver.
+ *
+ * Drop-in for the four task bodies of Charles-Chao-Chen/fastSolver's HODLR
+ * solve (paths relative to that project) plus the handle API that walks the
+ * tree the way FastSolver::bfs_solve does.
+ *
+ * Conventions
+ *   - Matrices are column-major FP64 with an explicit leading dimension, as the
+ *     reference's Legion regions are (raw_rect_ptr with LD == rows,
+ *     src/solver/solver_tasks.cc:408-410).
+ *   - Every pointer passed to a task body is a DEVICE pointer on the current
+ *     CUDA device; `stream` is a cudaStream_t passed as void* (NULL = legacy
+ *     default stream).
+ *   - Every call returns an int status: 0 = ok; > 0 = LAPACK-style INFO (the
+ *     1-based index of the first exactly-zero pivot); < 0 = bad argument
+ *     (-i: argument i is invalid) or one of the HODLR_ERR_* codes below.
+ *     The reference aborts via assert instead (solver_tasks.cc:284, 438, 516).
+ *   - Task bodies with an `info` argument are asynchronous when `info` is a
+ *     device pointer: they return after the launch and write INFO there.  When
+ *     `info` is NULL they synchronize `stream` and return INFO as the status.
+ *   - No entry point falls back to the CPU: without a usable CUDA device they
+ *     return HODLR_ERR_CUDA.
+ */
+#ifndef HODLR_GPU_H
+#define HODLR_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *hodlr_stream_t; /* cudaStream_t */
+
+#define HODLR_OK 0
+#define HODLR_ERR_CUDA (-1000)     /* CUDA runtime error / no device */
+#define HODLR_ERR_NOMEM (-1001)    /* device allocation failed */
+#define HODLR_ERR_STATE (-1002)    /* call out of order (e.g. solve before factor) */
+#define HODLR_ERR_NOCONV (-1003)   /* refinement did not reach the tolerance */
+#define HODLR_ERR_TIMEOUT (-1004)  /* a bounded device wait gave up */
+#define HODLR_ERR_UNSUPPORTED (-1005)
+
+#define HODLR_PREC_FP64 0  /* FP64 throughout (the reference's arithmetic) */
+#define HODLR_PREC_MIXED 1 /* FP32 leaf LU + split-BF16 tensor-core GEMMs,
+                              FP64 node LU, residual and refinement */
+
+/* ------------------------------------------------------------------------ */
+/* Task bodies                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* Leaf solve: dgesv of one leaf block on all its columns [b | U_anc].
+ * D (n x n, ldd) is overwritten by P*L*U (LAPACK dgetrf layout), X
+ * (n x nrhs, ldx) by D^{-1} X, ipiv (n ints, device) by LAPACK pivots (1-based).
+ * Replaces LeafSolveTask::cpu_task, real-leaf branch:
+ *   src/solver/solver_tasks.cc:341-412 (task), 424-450 (dgesv at 437). */
+int hodlr_leaf_solve(int n, int nrhs, double *D, int ldd, double *X, int ldx,
+                     int *ipiv, int *info, hodlr_stream_t stream);
+
+/* Upward reduce: W(r x ncol) += alpha * V(k x r)^T * U[:, col_beg:col_beg+ncol].
+ * U is k x (col_beg+ncol) (ldu).  Replaces GEMM_Reduce_Task::cpu_task:
+ *   src/solver/gemm.cc:315-384 (dgemm at 376; beta = 1 into the REDOP_ADD
+ *   region, which gemm_reduce zeroes first, gemm.cc:216-221). */
+int hodlr_gemm_reduce(double alpha, int k, int r, int ncol, const double *V,
+                      int ldv, const double *U, int ldu, int col_beg,
+                      double *W, int ldw, hodlr_stream_t stream);
+
+/* Node solve, r x r reduced Schur form.  V0Tu0 is r1 x r0, V1Tu1 r0 x r1,
+ * V0Td0 r1 x c, V1Td1 r0 x c:
+ *   V1Td1 -= V1Tu1 V0Td0;  S = I - V1Tu1 V0Tu0;  V1Td1 <- eta0 = S^{-1} V1Td1;
+ *   V0Td0 <- eta1 = V0Td0 - V0Tu0 eta0.
+ * Replaces LUSolveTask::cpu_task: src/solver/solver_tasks.cc:139-305. */
+int hodlr_node_lu_solve(int r0, int r1, int c, const double *V0Tu0, int ld00,
+                        const double *V1Tu1, int ld11, double *V0Td0,
+                        int ld0d, double *V1Td1, int ld1d, int *info,
+                        hodlr_stream_t stream);
+
+/* Node solve, 2r x 2r permuted Schur form [[V0Tu0, I], [I, V1Tu1]] with
+ * right-hand side [V0Td0; V1Td1]; on return V0Td0 <- eta0 (first r0 rows of
+ * the solution), V1Td1 <- eta1.  Replaces the leaf-internal branch of
+ * serial_leaf_solve: src/solver/solver_tasks.cc:483-535 (dgesv at 515).
+ * Uniform rank (r0 == r1) as in the reference's HodlrMatrix. */
+int hodlr_node_schur2_solve(int r0, int r1, int c, const double *V0Tu0,
+                            int ld00, const double *V1Tu1, int ld11,
+                            double *V0Td0, int ld0d, double *V1Td1, int ld1d,
+                            int *info, hodlr_stream_t stream);
+
+/* Downward broadcast: X[:, d_col_beg:d_col_beg+c] =
+ *   beta * X[:, d_col_beg:...] + alpha * X[:, u_col_beg:u_col_beg+r] * eta(r x c)
+ * on one k-row region X (ldx); the u and d column ranges must not overlap.
+ * Replaces GEMM_Broadcast_Task::cpu_task: src/solver/gemm.cc:417-478 (dgemm at
+ * 473; the solver calls it with alpha = -1, beta = 1, fast_solver.cc:250-253). */
+int hodlr_gemm_broadcast(double alpha, double beta, int k, int r, int c,
+                         double *X, int ldx, int u_col_beg, const double *eta,
+                         int lde, int d_col_beg, hodlr_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched (per-level) task bodies                                          */
+/* ------------------------------------------------------------------------ */
+
+/* One leaf of a batched leaf solve (device-resident array of these). */
+typedef struct {
+  double *D;  /* n x n, ldd */
+  double *X;  /* n x nrhs, ldx */
+  int *ipiv;  /* n ints */
+  int *perm;  /* n ints: final row order (row i of P^T D is row perm[i]) */
+  long long ldd;
+  long long ldx;
+  int n;
+  int nrhs;
+} hodlr_leaf_desc;
+
+/* All leaves of a level (or of many systems) in one launch pair.  `descs` is
+ * a device array of `count` descriptors, max_n the largest n among them;
+ * info (device, `count` ints) receives each leaf's INFO.  Asynchronous.
+ * Batched form of solver_tasks.cc:424-450 over the leaves that
+ * fast_solver.cc:197-201 visits. */
+int hodlr_leaf_solve_batched(int count, const hodlr_leaf_desc *descs,
+                             int max_n, int max_nrhs, int *info,
+                             hodlr_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Handle API: the solver that walks the tree (FastSolver + HodlrMatrix)     */
+/* ------------------------------------------------------------------------ */
+
+typedef struct hodlr_system_s *hodlr_system;
+
+/* Host-only: build the tree hodlr_create would build and write its node
+ * records (10 ints each, BFS order, see hodlr_tree_nodes) into `out`.
+ * Returns the node count, or < 0 (bad argument / cap too small = -6).
+ * Restates src/htree/hodlr_matrix.cc:138-169 and 354-386; needs no GPU. */
+int hodlr_build_tree(int N, int nrhs, int rank, int threshold, int *out,
+                     int cap);
+
+/* Build the HODLR tree of one N x N system with nrhs right-hand sides, rank r
+ * at every level and dense leaves of at most `threshold` rows (N/2, N - N/2
+ * split; leafSize = 1).  Mirrors HodlrMatrix::HodlrMatrix + create_tree:
+ * src/htree/hodlr_matrix.cc:22-33, 44-82, 138-169, 354-472.  Allocates the
+ * system's device arrays on the current device. */
+int hodlr_create(hodlr_system *sys, int N, int nrhs, int rank, int threshold);
+int hodlr_destroy(hodlr_system sys);
+
+/* Tree shape: node count, max depth, leaf count, total columns C = m + r*L,
+ * largest leaf.  Any output pointer may be NULL. */
+int hodlr_tree_info(hodlr_system sys, int *nnodes, int *max_depth,
+                    int *nleaves, int *ncols, int *max_leaf);
+/* Node records, 10 ints each in BFS order (nrow, ncol, row_beg, col_beg,
+ * lchild, rchild, parent, depth, vncol, is_leaf), into host array `out`. */
+int hodlr_tree_nodes(hodlr_system sys, int *out, int cap);
+
+/* Matrix data in the global layout: D (N x max_leaf, leaf blocks stacked),
+ * U and V (N x (C - m), column block of node c at c.col_beg - m), B (N x m).
+ * `host` != 0: the pointers are host memory (copied synchronously on
+ * `stream`); 0: device memory (copied device-to-device).  Any may be NULL to
+ * leave that part unchanged. */
+int hodlr_set_matrix(hodlr_system sys, const double *D, long long ldd,
+                     const double *U, long long ldu, const double *V,
+                     long long ldv, int host, hodlr_stream_t stream);
+int hodlr_set_rhs(hodlr_system sys, const double *B, long long ldb, int host,
+                  hodlr_stream_t stream);
+/* Copy the system's D, U, V, B out (same layouts; NULL skips a part). */
+int hodlr_get_matrix(hodlr_system sys, double *D, long long ldd, double *U,
+                     long long ldu, double *V, long long ldv, double *B,
+                     long long ldb, int host, hodlr_stream_t stream);
+
+/* Device-side generators.  hodlr_init_circulant: the reference's test matrix
+ * A = diag*I + U U^T, U(i, j) = (i + j) mod r (init_matrix_tasks.cc:176-219,
+ * hodlr_matrix.cc:528-567); hodlr_init_rhs_drand48: drand48_r(seed) stream
+ * reseeded per leaf, row-major fill (init_matrix_tasks.cc:43-77);
+ * hodlr_init_gaussian: leaf blocks G/sqrt(n) + 2I, U,V iid
+ * N(0,1)/sqrt(r n_child) rescaled so every off-diagonal block has spectral
+ * norm `offdiag_norm`, b iid N(0,1) (Philox4x32-10 counter RNG). */
+int hodlr_init_circulant(hodlr_system sys, double diag, hodlr_stream_t stream);
+int hodlr_init_rhs_drand48(hodlr_system sys, long seed, hodlr_stream_t stream);
+int hodlr_init_gaussian(hodlr_system sys, unsigned long long seed,
+                        double offdiag_norm, hodlr_stream_t stream);
+
+/* Fused FP64 factor+solve of the current RHS, the reference's bfs_solve
+ * (src/solver/fast_solver.cc:56-72, 136-255): leaf solves on [b | U], then per
+ * level 4 reduces -> node LU -> 2 broadcasts.  The solution is left in the
+ * system (hodlr_get_solution).  Asynchronous unless `sync`. */
+int hodlr_solve_fused(hodlr_system sys, int schur2, int sync,
+                      hodlr_stream_t stream);
+
+/* Factor/solve split (no reference counterpart: the reference always fuses).
+ * hodlr_factor keeps the leaf LU, the transformed U blocks and every node's
+ * capacitance LU in `precision`; hodlr_solve applies them to the current RHS. */
+int hodlr_factor(hodlr_system sys, int precision, hodlr_stream_t stream);
+int hodlr_solve(hodlr_system sys, hodlr_stream_t stream);
+
+/* Mixed-precision solve with FP64 iterative refinement until
+ * max_j ||b_j - A x_j|| / ||b_j|| <= tol (or maxiter sweeps).  One call =
+ * factor (FP32, carrying b) + refinement sweeps; iters and relres (host
+ * pointers, may be NULL) report the result.  Returns HODLR_ERR_NOCONV if
+ * the tolerance was not met. */
+int hodlr_solve_refined(hodlr_system sys, int precision, double tol,
+                        int maxiter, int *iters, double *relres,
+                        hodlr_stream_t stream);
+
+/* y = A x (FP64 HODLR matvec) for x, y device arrays N x ncols (ldx, ldy),
+ * ncols <= nrhs. */
+int hodlr_matvec(hodlr_system sys, const double *x, long long ldx, double *y,
+                 long long ldy, int ncols, hodlr_stream_t stream);
+
+/* max_j ||b_j - A x_j||_2 / ||b_j||_2 of the current solution (host result). */
+int hodlr_relres(hodlr_system sys, double *relres, hodlr_stream_t stream);
+
+/* Copy the solution (N x m) out: host != 0 -> host memory. */
+int hodlr_get_solution(hodlr_system sys, double *X, long long ldx, int host,
+                       hodlr_stream_t stream);
+
+/* Per-phase device time.  While profiling is on (off by default), every
+ * launch group is bracketed by CUDA events; hodlr_phase_times synchronizes
+ * and returns, per phase, the accumulated milliseconds and the number of
+ * launches since the last reset (ms / launches: arrays of HODLR_PHASES,
+ * either may be NULL).  Phases: 0 getrf, 1 getrs, 2 reduce, 3 node factor,
+ * 4 node apply, 5 broadcast, 6 matvec, 7 precision conversion. */
+#define HODLR_PHASES 8
+int hodlr_set_profiling(hodlr_system sys, int on);
+int hodlr_phase_times(hodlr_system sys, double *ms, long long *launches,
+                      int reset);
+
+/* Number of kernels this library launched on this thread since the last
+ * reset (every launch from a hodlr_* call is counted). */
+long long hodlr_launch_count(void);
+void hodlr_reset_launch_count(void);
+
+/* Human-readable text of a status code. */
+const char *hodlr_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HODLR_GPU_H */
