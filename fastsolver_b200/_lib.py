@@ -49,6 +49,7 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _SIGS = {
     "hodlr_leaf_solve": [_i, _i, _vp, _i, _vp, _i, _vp, _vp, _vp],
     "hodlr_gemm_reduce": [_d, _i, _i, _i, _vp, _i, _vp, _i, _i, _vp, _i, _vp],
+    "hodlr_gemm_reduce_noalloc": [_d, _i, _i, _i, _vp, _i, _vp, _i, _i, _vp, _i, _vp],
     "hodlr_node_lu_solve": [_i, _i, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp],
     "hodlr_node_schur2_solve": [_i, _i, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _i, _vp, _vp],
     "hodlr_gemm_broadcast": [_d, _d, _i, _i, _i, _vp, _i, _i, _vp, _i, _i, _vp],

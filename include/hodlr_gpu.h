@@ -63,6 +63,22 @@ int hodlr_gemm_reduce(double alpha, int k, int r, int ncol, const double *V,
                       int ldv, const double *U, int ldu, int col_beg,
                       double *W, int ldw, hodlr_stream_t stream);
 
+/* Same result as hodlr_gemm_reduce, allocating no device memory: for callers
+ * that cannot allocate, e.g. task bodies under a runtime that owns the GPU's
+ * memory (Legion/Realm reserves the framebuffer and hands tasks only mapped
+ * regions) or services that pre-reserve all device memory.  No counterpart in
+ * the reference.  Its split-K partial sums live in a fixed 8 MiB array in the
+ * library's device image (held by every GPU that loads the library until the
+ * process exits); r * ncol must not exceed 2^20, else the call returns
+ * HODLR_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race.
+ * Asynchronous on `stream`. */
+int hodlr_gemm_reduce_noalloc(double alpha, int k, int r, int ncol,
+                              const double *V, int ldv, const double *U,
+                              int ldu, int col_beg, double *W, int ldw,
+                              hodlr_stream_t stream);
+
 /* Node solve, r x r reduced Schur form.  V0Tu0 is r1 x r0, V1Tu1 r0 x r1,
  * V0Td0 r1 x c, V1Td1 r0 x c:
  *   V1Td1 -= V1Tu1 V0Td0;  S = I - V1Tu1 V0Tu0;  V1Td1 <- eta0 = S^{-1} V1Td1;
