@@ -235,16 +235,24 @@ static int node_solve_common(int form, int r0, int r1, int c, const double *V0Tu
   if (int e = device_ok()) return e;
   return guarded([&]() -> int {
     cudaStream_t s = as_stream(stream);
-    const size_t need = sizeof(double) * ((size_t)s_ * s_ + 2 * (size_t)r0 * r1) +
-                        sizeof(int) * (s_ + 8) + sizeof(NodeTask<double, double>) + 1024;
+    // scratch: task | S (s x s) | S^{-1} (s x s) | I (s x s) | VTu0 | VTu1 | piv | info
+    //          | gram item + segment
+    const size_t nS = (size_t)s_ * s_;
+    const size_t need = 256 + sizeof(double) * (3 * nS + 2 * (size_t)r0 * r1) +
+                        sizeof(int) * (s_ + 8) + 512;
     StreamScratch scr(need, s);
     char *base = static_cast<char *>(scr.p);
     auto *task = reinterpret_cast<NodeTask<double, double> *>(base);
     double *S_lu = reinterpret_cast<double *>(base + 256);
-    double *VTu0 = S_lu + (size_t)s_ * s_;
+    double *S_inv = S_lu + nS;
+    double *ident = S_inv + nS;
+    double *VTu0 = ident + nS;
     double *VTu1 = VTu0 + (size_t)r0 * r1;
     int *piv = reinterpret_cast<int *>(VTu1 + (size_t)r0 * r1);
     int *info_dev = info ? info : piv + s_;
+    auto *gitem = reinterpret_cast<GemmItem<double, double> *>(
+        (reinterpret_cast<uintptr_t>(piv + s_ + 8) + 15) & ~uintptr_t(15));
+    auto *gseg = reinterpret_cast<GemmSeg<double> *>(gitem + 1);
     NodeTask<double, double> k{};
     k.W0d = V0Td0; k.W0u = V0Tu0; k.W1d = V1Td1; k.W1u = V1Tu1;
     k.w0_stride = k.w1_stride = 0;
@@ -255,9 +263,21 @@ static int node_solve_common(int form, int r0, int r1, int c, const double *V0Tu
     // (fast_solver.cc:238-240); form 1 eta0 over V0Td0, eta1 over V1Td1.
     if (form == 0) { k.eta0 = V1Td1; k.ld_eta0 = ld1d; k.eta1 = V0Td0; k.ld_eta1 = ld0d; }
     else { k.eta0 = V0Td0; k.ld_eta0 = ld0d; k.eta1 = V1Td1; k.ld_eta1 = ld1d; }
-    k.S_lu = S_lu; k.S_piv = piv; k.VTu0 = VTu0; k.VTu1 = VTu1;
+    k.S_lu = S_lu; k.S_inv = S_inv; k.S_piv = piv; k.VTu0 = VTu0; k.VTu1 = VTu1;
     k.info_slot = 0;
     HODLR_CUDA_TRY(cudaMemcpyAsync(task, &k, sizeof(k), cudaMemcpyHostToDevice, s));
+    if (form == 0) {
+      // S = I - V1Tu1 V0Tu0 into S_lu (the dgemm at solver_tasks.cc:261)
+      std::vector<double> I(nS, 0.0);
+      for (int i = 0; i < s_; ++i) I[(size_t)i * s_ + i] = 1.0;
+      HODLR_CUDA_TRY(cudaMemcpyAsync(ident, I.data(), sizeof(double) * nS, cudaMemcpyHostToDevice, s));
+      GemmSeg<double> g{V1Tu1, V0Tu0, ld11, ld00, r1, 0};
+      GemmItem<double, double> it{S_lu, ident, r0, s_, r0, r0, 0, 1};
+      HODLR_CUDA_TRY(cudaMemcpyAsync(gitem, &it, sizeof(it), cudaMemcpyHostToDevice, s));
+      HODLR_CUDA_TRY(cudaMemcpyAsync(gseg, &g, sizeof(g), cudaMemcpyHostToDevice, s));
+      launch_gemm_items<double, double, double>(gitem, gseg, 1, r0, r0, false, -1.0, 1.0, s);
+      HODLR_CUDA_TRY(cudaStreamSynchronize(s));  // host staging buffers go out of scope
+    }
     launch_node_factor<double, double>(task, 1, s_, form, info_dev, s);
     if (c > 0) launch_node_apply<double, double>(task, 1, s_, r0 + r1, c, form, s);
     int rc = finish_info(info, info_dev, s);

@@ -112,8 +112,9 @@ struct NodeTask {
   TE *eta0;           // r0 x c out, ld ld_eta0: broadcast into child 0
   TE *eta1;           // r1 x c out, ld ld_eta1: broadcast into child 1
   long long ld_eta0, ld_eta1;
-  double *S_lu;       // s x s LU of the capacitance matrix (s = r0 or r0+r1)
+  double *S_lu;       // s x s: S before factoring (form 0), then its LU
   int *S_piv;         // s, 0-based pivot rows
+  double *S_inv;      // s x s: S^{-1} from the LU factors
   double *VTu0;       // r1 x r0: V0^T u0 (factor writes, apply reads)
   double *VTu1;       // r0 x r1: V1^T u1
   int np0, np1;

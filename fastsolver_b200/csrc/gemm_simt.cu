@@ -115,6 +115,148 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Skinny items (N <= 32 columns: the m right-hand sides of the matvec and of
+// the refinement sweeps).  These are bandwidth-bound, so the kernels aim at
+// bytes in flight rather than register tiles.
+// ---------------------------------------------------------------------------
+
+// NN: one thread per output row, N accumulators; B's rows staged in shared
+// memory (broadcast reads), A streamed with 8 loads in flight per thread.
+template <typename TA, typename TC, typename TACC, int NC>
+__global__ void __launch_bounds__(NT)
+    skinny_nn_kernel(const GemmItem<TA, TC> *__restrict__ items,
+                     const GemmSeg<TA> *__restrict__ segs, TACC alpha, TACC beta) {
+  constexpr int KT = 64;
+  __shared__ __align__(16) TACC Bs[KT * NC];
+  const GemmItem<TA, TC> it = items[blockIdx.x];
+  const int m0 = blockIdx.y * NT;
+  if (m0 >= it.M) return;
+  const int tid = threadIdx.x;
+  const int row = m0 + tid;
+  TACC acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c] = TACC(0);
+  for (int s = it.seg_begin; s < it.seg_begin + it.seg_count; ++s) {
+    const GemmSeg<TA> sg = segs[s];
+    for (int k0 = 0; k0 < sg.K; k0 += KT) {
+      const int kt = min(KT, sg.K - k0);
+      for (int e = tid; e < KT * NC; e += NT) {
+        const int kk = e % KT, c = e / KT;
+        Bs[kk * NC + c] = (kk < kt && c < it.N) ? TACC(sg.B[(k0 + kk) + (long long)c * sg.ldb])
+                                                : TACC(0);
+      }
+      __syncthreads();
+      if (row < it.M) {
+        const TA *a = sg.A + row + (long long)k0 * sg.lda;
+        int kk = 0;
+        for (; kk + 8 <= kt; kk += 8) {
+          TACC av[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) av[u] = TACC(a[(long long)(kk + u) * sg.lda]);
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) acc[c] += av[u] * Bs[(kk + u) * NC + c];
+        }
+        for (; kk < kt; ++kk) {
+          const TACC av = TACC(a[(long long)kk * sg.lda]);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) acc[c] += av * Bs[kk * NC + c];
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (row < it.M) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if (c >= it.N) break;
+      TACC v = alpha * acc[c];
+      if (it.Cin) v += beta * TACC(it.Cin[row + (long long)c * it.ldcin]);
+      it.C[row + (long long)c * it.ldc] = TC(v);
+    }
+  }
+}
+
+// TN: C (64 x 16 tile) = A^T B over the item's K rows.  Tiles of 64 rows are
+// staged in shared memory; warp w takes rows w, w+8, ... of each tile with a
+// 4 x 8 register tile per lane; the 8 warp partials are summed at the end.
+template <typename TA, typename TC, typename TACC>
+__global__ void __launch_bounds__(NT)
+    skinny_tn_kernel(const GemmItem<TA, TC> *__restrict__ items,
+                     const GemmSeg<TA> *__restrict__ segs, TACC alpha, TACC beta) {
+  constexpr int TM = 64, TNc = 16, KT = 64;
+  __shared__ __align__(16) TACC As[KT * TM];
+  __shared__ __align__(16) TACC Bs[KT * TNc];
+  extern __shared__ __align__(16) unsigned char red_raw[];
+  TACC *red = reinterpret_cast<TACC *>(red_raw);  // 8 x (TM * TNc)
+  const GemmItem<TA, TC> it = items[blockIdx.x];
+  const int m0 = blockIdx.y * TM, n0 = blockIdx.z * TNc;
+  if (m0 >= it.M || n0 >= it.N) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int mg = lane & 15, ng = lane >> 4;  // m = mg*4.., n = ng*8..
+  TACC acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = TACC(0);
+  for (int s = it.seg_begin; s < it.seg_begin + it.seg_count; ++s) {
+    const GemmSeg<TA> sg = segs[s];
+    for (int k0 = 0; k0 < sg.K; k0 += KT) {
+      // A tile: rows k0.., columns m0..m0+63; threads run along k (coalesced)
+#pragma unroll
+      for (int u = 0; u < KT * TM / NT; ++u) {
+        const int e = tid + u * NT;
+        const int kk = e % KT, mm = e / KT;
+        const int gk = k0 + kk, gm = m0 + mm;
+        As[kk * TM + mm] =
+            (gk < sg.K && gm < it.M) ? TACC(sg.A[gk + (long long)gm * sg.lda]) : TACC(0);
+      }
+#pragma unroll
+      for (int u = 0; u < KT * TNc / NT; ++u) {
+        const int e = tid + u * NT;
+        const int kk = e % KT, nn = e / KT;
+        const int gk = k0 + kk, gn = n0 + nn;
+        Bs[kk * TNc + nn] =
+            (gk < sg.K && gn < it.N) ? TACC(sg.B[gk + (long long)gn * sg.ldb]) : TACC(0);
+      }
+      __syncthreads();
+#pragma unroll 2
+      for (int kk = warp; kk < KT; kk += 8) {
+        TACC a[4], b[8];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[kk * TM + mg * 4 + i];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) b[j] = Bs[kk * TNc + ng * 8 + j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc[i][j] += a[i] * b[j];
+      }
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      red[warp * (TM * TNc) + (ng * 8 + j) * TM + mg * 4 + i] = acc[i][j];
+  __syncthreads();
+  for (int e = tid; e < TM * TNc; e += NT) {
+    const int mm = e % TM, nn = e / TM;
+    const int gm = m0 + mm, gn = n0 + nn;
+    if (gm >= it.M || gn >= it.N) continue;
+    TACC v = TACC(0);
+#pragma unroll
+    for (int w = 0; w < 8; ++w) v += red[w * (TM * TNc) + e];
+    v *= alpha;
+    if (it.Cin) v += beta * TACC(it.Cin[gm + (long long)gn * it.ldcin]);
+    it.C[gm + (long long)gn * it.ldc] = TC(v);
+  }
+}
+
 }  // namespace
 
 template <typename TA, typename TC, typename TACC>
@@ -123,11 +265,19 @@ void launch_gemm_items(const GemmItem<TA, TC> *items, const GemmSeg<TA> *segs, i
                        cudaStream_t s) {
   if (nitems <= 0 || max_m <= 0 || max_n <= 0) return;
   if (max_n <= 32) {
-    dim3 grid(nitems, cdiv(max_m, BM), cdiv(max_n, 32));
-    if (trans)
-      gemm_items_kernel<TA, TC, TACC, true, 2><<<grid, NT, 0, s>>>(items, segs, alpha, beta);
-    else
-      gemm_items_kernel<TA, TC, TACC, false, 2><<<grid, NT, 0, s>>>(items, segs, alpha, beta);
+    if (trans) {
+      dim3 grid(nitems, cdiv(max_m, 64), cdiv(max_n, 16));
+      const size_t red = 8 * 64 * 16 * sizeof(TACC);
+      HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_tn_kernel<TA, TC, TACC>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)red));
+      skinny_tn_kernel<TA, TC, TACC><<<grid, NT, red, s>>>(items, segs, alpha, beta);
+    } else {
+      dim3 grid(nitems, cdiv(max_m, NT));
+      if (max_n <= 16)
+        skinny_nn_kernel<TA, TC, TACC, 16><<<grid, NT, 0, s>>>(items, segs, alpha, beta);
+      else
+        skinny_nn_kernel<TA, TC, TACC, 32><<<grid, NT, 0, s>>>(items, segs, alpha, beta);
+    }
   } else {
     dim3 grid(nitems, cdiv(max_m, BM), cdiv(max_n, 128));
     if (trans)
@@ -142,6 +292,9 @@ template void launch_gemm_items<double, double, double>(const GemmItem<double, d
                                                         const GemmSeg<double> *, int, int,
                                                         int, bool, double, double,
                                                         cudaStream_t);
+template void launch_gemm_items<float, double, double>(const GemmItem<float, double> *,
+                                                       const GemmSeg<float> *, int, int, int,
+                                                       bool, double, double, cudaStream_t);
 template void launch_gemm_items<float, float, float>(const GemmItem<float, float> *,
                                                      const GemmSeg<float> *, int, int, int,
                                                      bool, float, float, cudaStream_t);

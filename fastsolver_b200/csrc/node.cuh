@@ -8,7 +8,7 @@ namespace hodlr {
 constexpr int kMaxNodeS = 144;
 
 size_t node_factor_smem(int max_s);
-size_t node_apply_smem(int max_s, int max_rs);
+size_t node_apply_smem(int max_s, int max_rs, int form);
 
 // One CTA per node: V^T u sums, S formation and LU (writes S_lu, S_piv, VTu*).
 template <typename TW, typename TE>

@@ -39,30 +39,41 @@ struct PathSpec {
   int *ipiv = nullptr, *perm = nullptr;
   const T *V = nullptr;
   long long ldv = 0;
-  T *part = nullptr;
+  T *part = nullptr;   // split-K partial slots
+  T *wfin = nullptr;   // summed W per child (when a child has several slots)
   TE *eta = nullptr;
   NodeStore *ns = nullptr;
   bool factor = false;
   int red_chunk = 512, bc_chunk = 512;
 };
 
-// Partial-sum and eta workspace (elements) a path needs at its largest level.
-void path_need(const Tree &t, bool factor, int chunk, size_t &part, size_t &eta) {
-  part = 0;
-  eta = 0;
+// Rows per split-K slot of a child with `nrow` rows: at least `chunk` rows,
+// at most kMaxSlots slots (the node kernels read one summed W per child).
+constexpr int kMaxSlots = 64;
+inline int slot_rows(int nrow, int chunk) {
+  const int ns = std::max(1, std::min(cdiv(nrow, chunk), kMaxSlots));
+  return cdiv(cdiv(nrow, ns), 16) * 16;
+}
+
+// Partial-sum, summed-W and eta workspace (elements) of a path's largest level.
+void path_need(const Tree &t, bool factor, int chunk, size_t &part, size_t &wfin, size_t &eta) {
+  part = wfin = eta = 0;
   for (int d = t.max_depth - 1; d >= 0; --d) {
-    size_t p = 0, e = 0;
+    size_t p = 0, w = 0, e = 0;
     for (int id : t.internal_at_depth[d]) {
       const Node &P = t.nodes[id];
       const Node &c0 = t.nodes[P.lchild], &c1 = t.nodes[P.rchild];
       const int cw = factor ? c0.col_beg : t.nrhs;
       for (const Node *c : {&c0, &c1}) {
         const int NW = factor ? c->col_beg + c->ncol : t.nrhs;
-        p += (size_t)cdiv(c->nrow, chunk) * c->vncol * NW;
+        const int ns = cdiv(c->nrow, slot_rows(c->nrow, chunk));
+        p += (size_t)ns * c->vncol * NW;
+        if (ns > 1) w += (size_t)c->vncol * NW;
       }
       e += (size_t)(c0.ncol + c1.ncol) * cw;
     }
     part = std::max(part, p);
+    wfin = std::max(wfin, w);
     eta = std::max(eta, e);
   }
 }
@@ -101,7 +112,10 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
     std::vector<GemmItem<T, T>> ri, bi;
     std::vector<GemmSeg<T>> rs, bs;
     std::vector<NodeTask<T, TE>> nt;
-    size_t poff = 0, eoff = 0;
+    std::vector<SumTask<T>> su;
+    std::vector<GemmItem<T, double>> gi;
+    std::vector<GemmSeg<T>> gs;
+    size_t poff = 0, woff = 0, eoff = 0;
     for (int p : ids) {
       const Node &P = t.nodes[p];
       const Node &c0 = t.nodes[P.lchild], &c1 = t.nodes[P.rchild];
@@ -111,11 +125,12 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
         const Node &c = side ? c1 : c0;
         const int NW = sp.factor ? c.col_beg + c.ncol : m;
         const int M = c.vncol;
-        const int nslots = cdiv(c.nrow, sp.red_chunk);
+        const int rows_per = slot_rows(c.nrow, sp.red_chunk);
+        const int nslots = cdiv(c.nrow, rows_per);
         T *slot0 = sp.part + poff;
         for (int q = 0; q < nslots; ++q) {
-          const int rb = c.row_beg + q * sp.red_chunk;
-          const int rows = std::min(sp.red_chunk, c.row_beg + c.nrow - rb);
+          const int rb = c.row_beg + q * rows_per;
+          const int rows = std::min(rows_per, c.row_beg + c.nrow - rb);
           GemmSeg<T> sg{};
           sg.A = sp.V + rb + (long long)(c.col_beg - m) * sp.ldv;
           sg.B = sp.X + rb;
@@ -136,12 +151,25 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
           L->red_max_n = std::max(L->red_max_n, NW);
         }
         poff += (size_t)nslots * M * NW;
+        T *W = slot0;
+        if (nslots > 1) {
+          W = sp.wfin + woff;
+          woff += (size_t)M * NW;
+          SumTask<T> st{};
+          st.dst = W;
+          st.src = slot0;
+          st.len = (long long)M * NW;
+          st.stride = (long long)M * NW;
+          st.nslots = nslots;
+          su.push_back(st);
+          L->sum_max_len = std::max(L->sum_max_len, st.len);
+        }
         if (side == 0) {
-          k.W0d = slot0; k.W0u = slot0 + (size_t)M * (NW - c.ncol);
-          k.w0_stride = (long long)M * NW; k.ldw0d = k.ldw0u = M; k.np0 = nslots;
+          k.W0d = W; k.W0u = W + (size_t)M * (NW - c.ncol);
+          k.ldw0d = k.ldw0u = M; k.np0 = 1;
         } else {
-          k.W1d = slot0; k.W1u = slot0 + (size_t)M * (NW - c.ncol);
-          k.w1_stride = (long long)M * NW; k.ldw1d = k.ldw1u = M; k.np1 = nslots;
+          k.W1d = W; k.W1u = W + (size_t)M * (NW - c.ncol);
+          k.ldw1d = k.ldw1u = M; k.np1 = 1;
         }
       }
       k.r0 = c0.ncol;
@@ -154,11 +182,32 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
       k.ld_eta1 = k.r1;
       eoff += (size_t)k.r1 * cw;
       k.S_lu = sp.ns->S_lu.p + (size_t)p * sp.ns->s_slot;
+      k.S_inv = sp.ns->S_inv.p + (size_t)p * sp.ns->s_slot;
       k.S_piv = sp.ns->S_piv.p + (size_t)p * sp.ns->s_max;
       k.VTu0 = sp.ns->VTu0.p + (size_t)p * sp.ns->rr;
       k.VTu1 = sp.ns->VTu1.p + (size_t)p * sp.ns->rr;
       k.info_slot = nleaf + p;
       nt.push_back(k);
+      if (sp.factor && form == 0) {
+        // S = I - V1Tu1 V0Tu0 (r0 x r0, ld r0) into the node's S_lu slot
+        GemmSeg<T> g{};
+        g.A = k.W1u;
+        g.lda = k.ldw1u;
+        g.B = k.W0u;
+        g.ldb = k.ldw0u;
+        g.K = k.r1;
+        GemmItem<T, double> it{};
+        it.C = k.S_lu;
+        it.ldc = k.r0;
+        it.Cin = sp.ns->ident.p;
+        it.ldcin = sp.ns->s_max;
+        it.M = it.N = k.r0;
+        it.seg_begin = (int)gs.size();
+        it.seg_count = 1;
+        gs.push_back(g);
+        gi.push_back(it);
+        L->gram_max = std::max(L->gram_max, k.r0);
+      }
       const int s = form == 0 ? k.r0 : k.r0 + k.r1;
       L->max_s = std::max(L->max_s, s);
       L->max_rs = std::max(L->max_rs, k.r0 + k.r1);
@@ -194,6 +243,11 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
     L->red_items.upload(ri);
     L->red_segs.upload(rs);
     L->n_red = (int)ri.size();
+    L->sums.upload(su);
+    L->n_sums = (int)su.size();
+    L->gram_items.upload(gi);
+    L->gram_segs.upload(gs);
+    L->n_gram = (int)gi.size();
     L->node_tasks.upload(nt);
     L->n_nodes = (int)nt.size();
     L->bc_items.upload(bi);
@@ -235,9 +289,13 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
       PhaseScope ps(pf, PH_REDUCE, s);
       launch_gemm_items<T, T, T>(L.red_items.p, L.red_segs.p, L.n_red, L.red_max_m,
                                  L.red_max_n, true, T(1), T(0), s);
+      launch_sum_slots<T>(L.sums.p, L.n_sums, L.sum_max_len, s);
     }
     if (plan.factor) {
       PhaseScope ps(pf, PH_NODE_FACTOR, s);
+      if (form == 0)
+        launch_gemm_items<T, double, double>(L.gram_items.p, L.gram_segs.p, L.n_gram, L.gram_max,
+                                             L.gram_max, false, -1.0, 1.0, s);
       launch_node_factor<T, TE>(L.node_tasks.p, L.n_nodes, L.max_s, form, info, s);
     }
     {
@@ -259,7 +317,11 @@ void alloc_node_store(NodeStore &ns, const Tree &t) {
   ns.rr = r * r;
   const size_t nn = t.nodes.size();
   ns.S_lu.ensure(nn * ns.s_slot);
+  ns.S_inv.ensure(nn * ns.s_slot);
   ns.S_piv.ensure(nn * ns.s_max);
+  std::vector<double> I((size_t)ns.s_max * ns.s_max, 0.0);
+  for (int i = 0; i < ns.s_max; ++i) I[(size_t)i * ns.s_max + i] = 1.0;
+  ns.ident.upload(I);
   ns.VTu0.ensure(nn * ns.rr);
   ns.VTu1.ensure(nn * ns.rr);
 }
@@ -268,7 +330,7 @@ void build_matvec(System &S, const double *x, MatvecPlan &mv) {
   const Tree &t = S.tree;
   const int m = S.m;
   const long long N = S.N;
-  const int chunk = 2048;
+  const int chunk = 1024;
   std::vector<GemmItem<double, double>> ri, ai;
   std::vector<GemmSeg<double>> rs, as;
   std::vector<SumTask<double>> su;
@@ -280,19 +342,22 @@ void build_matvec(System &S, const double *x, MatvecPlan &mv) {
     tsz += (size_t)c.vncol * m;
   }
   size_t pneed = 0;
-  for (size_t i = 1; i < t.nodes.size(); ++i)
-    pneed += (size_t)cdiv(t.nodes[i].nrow, chunk) * t.nodes[i].vncol * m;
+  for (size_t i = 1; i < t.nodes.size(); ++i) {
+    const int rp = slot_rows(t.nodes[i].nrow, chunk);
+    pneed += (size_t)cdiv(t.nodes[i].nrow, rp) * t.nodes[i].vncol * m;
+  }
   S.tbuf.ensure(std::max<size_t>(tsz, 1));
   S.mvpart.ensure(std::max<size_t>(pneed, 1));
   mv.red_max_m = mv.red_max_n = 0;
   for (size_t i = 1; i < t.nodes.size(); ++i) {
     const Node &c = t.nodes[i];
     const int M = c.vncol;
-    const int nslots = cdiv(c.nrow, chunk);
+    const int rows_per = slot_rows(c.nrow, chunk);
+    const int nslots = cdiv(c.nrow, rows_per);
     double *slot0 = S.mvpart.p + poff;
     for (int q = 0; q < nslots; ++q) {
-      const int rb = c.row_beg + q * chunk;
-      const int rows = std::min(chunk, c.row_beg + c.nrow - rb);
+      const int rb = c.row_beg + q * rows_per;
+      const int rows = std::min(rows_per, c.row_beg + c.nrow - rb);
       GemmSeg<double> sg{};
       sg.A = S.V.p + rb + (long long)(c.col_beg - m) * N;
       sg.B = x + rb;
@@ -438,17 +503,18 @@ void System::ensure_fp64() {
   ipiv64.ensure(n);
   perm64.ensure(n);
   alloc_node_store(ns64, tree);
-  size_t pf, ef, pa, ea;
-  path_need(tree, true, red_chunk, pf, ef);
-  path_need(tree, false, red_chunk, pa, ea);
+  size_t pf, wf, ef, pa, wa, ea;
+  path_need(tree, true, red_chunk, pf, wf, ef);
+  path_need(tree, false, red_chunk, pa, wa, ea);
   part64.ensure(std::max<size_t>(std::max(pf, pa), 1));
+  wfin64.ensure(std::max<size_t>(std::max(wf, wa), 1));
   eta64.ensure(std::max<size_t>(std::max(ef, ea), 1));
   for (int form = 0; form < 2; ++form) {
     if (form == 1 && ns64.s_max < 2 * r) continue;
     PathSpec<double, double> f;
     f.X = X64.p; f.ldx = N; f.Usrc = X64.p; f.ldu = N;
     f.D = DLU64.p; f.ldd = N; f.ipiv = ipiv64.p; f.perm = perm64.p;
-    f.V = V.p; f.ldv = N; f.part = part64.p; f.eta = eta64.p; f.ns = &ns64;
+    f.V = V.p; f.ldv = N; f.part = part64.p; f.wfin = wfin64.p; f.eta = eta64.p; f.ns = &ns64;
     f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk;
     build_path(tree, f, fused64[form], form);
     PathSpec<double, double> a = f;
@@ -467,15 +533,16 @@ void System::ensure_mixed() {
   ipiv32.ensure(n);
   perm32.ensure(n);
   alloc_node_store(ns32, tree);
-  size_t pf, ef, pa, ea;
-  path_need(tree, true, red_chunk, pf, ef);
-  path_need(tree, false, red_chunk, pa, ea);
+  size_t pf, wf, ef, pa, wa, ea;
+  path_need(tree, true, red_chunk, pf, wf, ef);
+  path_need(tree, false, red_chunk, pa, wa, ea);
   part32.ensure(std::max<size_t>(std::max(pf, pa), 1));
+  wfin32.ensure(std::max<size_t>(std::max(wf, wa), 1));
   eta32.ensure(std::max<size_t>(std::max(ef, ea), 1));
   PathSpec<float, float> f;
   f.X = X32.p; f.ldx = N; f.Usrc = X32.p; f.ldu = N;
   f.D = D32.p; f.ldd = N; f.ipiv = ipiv32.p; f.perm = perm32.p;
-  f.V = V32.p; f.ldv = N; f.part = part32.p; f.eta = eta32.p; f.ns = &ns32;
+  f.V = V32.p; f.ldv = N; f.part = part32.p; f.wfin = wfin32.p; f.eta = eta32.p; f.ns = &ns32;
   f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk;
   build_path(tree, f, fused32, 0);
   PathSpec<float, float> a = f;

@@ -47,6 +47,8 @@ struct DevBuf {
 // Per-node factorization data kept for solves with the same factors.
 struct NodeStore {
   DevBuf<double> S_lu;   // per node: s_slot doubles
+  DevBuf<double> S_inv;  // per node: s_slot doubles
+  DevBuf<double> ident;  // s_max x s_max identity (the I of S = I - V1Tu1 V0Tu0)
   DevBuf<int> S_piv;     // per node: s_max ints
   DevBuf<double> VTu0;   // per node: r*r
   DevBuf<double> VTu1;
@@ -58,6 +60,12 @@ struct LevelPlan {
   DevBuf<GemmItem<T, T>> red_items;
   DevBuf<GemmSeg<T>> red_segs;
   int n_red = 0, red_max_m = 0, red_max_n = 0;
+  DevBuf<SumTask<T>> sums;          // partial slots -> one W per child
+  int n_sums = 0;
+  long long sum_max_len = 0;
+  DevBuf<GemmItem<T, double>> gram_items;  // S = I - V1Tu1 V0Tu0, FP64 result
+  DevBuf<GemmSeg<T>> gram_segs;
+  int n_gram = 0, gram_max = 0;
   DevBuf<NodeTask<T, TE>> node_tasks;
   int n_nodes = 0, max_s = 0, max_rs = 0, max_c = 0;
   DevBuf<GemmItem<T, T>> bc_items;
@@ -118,8 +126,8 @@ struct System {
   DevBuf<int> ipiv32, perm32;
   DevBuf<double> R64, MVx, relres_dev;
   // workspaces
-  DevBuf<double> part64, eta64, tbuf, mvpart;
-  DevBuf<float> part32, eta32;
+  DevBuf<double> part64, wfin64, eta64, tbuf, mvpart;
+  DevBuf<float> part32, wfin32, eta32;
   DevBuf<int> info;
   NodeStore ns64, ns32;
   PathPlan<double, double> fused64[2];  // [form]

@@ -229,6 +229,7 @@ void launch_sum_slots(const SumTask<T> *tasks, int ntasks, long long max_len, cu
   HODLR_LAUNCH_CHECK();
 }
 template void launch_sum_slots<double>(const SumTask<double> *, int, long long, cudaStream_t);
+template void launch_sum_slots<float>(const SumTask<float> *, int, long long, cudaStream_t);
 
 void launch_scale_cols(double *a, long long lda, long long rows, int cols, const double *s_dev,
                        cudaStream_t s) {
