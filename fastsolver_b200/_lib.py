@@ -55,6 +55,8 @@ _SIGS = {
     "hodlr_gemm_broadcast": [_d, _d, _i, _i, _i, _vp, _i, _i, _vp, _i, _i, _vp],
     "hodlr_leaf_solve_batched": [_i, _vp, _i, _i, _vp, _vp],
     "hodlr_build_tree": [_i, _i, _i, _i, _ip, _i],
+    "hodlr_gemm_f32": [_i, _i, _i, _i, ctypes.c_float, _vp, _i, _vp, _i, ctypes.c_float, _vp, _i,
+                       _i, _vp],
     "hodlr_create": [ctypes.POINTER(_vp), _i, _i, _i, _i],
     "hodlr_destroy": [_vp],
     "hodlr_tree_info": [_vp, _ip, _ip, _ip, _ip, _ip],

@@ -9,6 +9,7 @@
 #include "leaf.cuh"
 #include "node.cuh"
 #include "solver.h"
+#include "tc_gemm.cuh"
 #include "util.cuh"
 
 namespace hodlr {
@@ -212,6 +213,40 @@ int hodlr_gemm_reduce(double alpha, int k, int r, int ncol, const double *V, int
     launch_add2d<double>(W, ldw, static_cast<double *>(tmp.p), r, r, ncol, s);
     HODLR_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
+  });
+}
+
+int hodlr_gemm_f32(int transa, int m, int n, int k, float alpha, const float *A, int lda,
+                   const float *B, int ldb, float beta, float *C, int ldc, int engine,
+                   hodlr_stream_t stream) {
+  if (transa != 0 && transa != 1) return -1;
+  if (m < 0) return -2;
+  if (n < 0) return -3;
+  if (k < 0) return -4;
+  if (!A && m > 0 && k > 0) return -6;
+  if (lda < std::max(1, transa ? k : m)) return -7;
+  if (!B && k > 0 && n > 0) return -8;
+  if (ldb < std::max(1, k)) return -9;
+  if (!C && m > 0 && n > 0) return -11;
+  if (ldc < std::max(1, m)) return -12;
+  if (engine != 0 && engine != 1) return -13;
+  if (int e = device_ok()) return e;
+  return guarded([&]() -> int {
+    if (m == 0 || n == 0) return 0;
+    cudaStream_t s = as_stream(stream);
+    GemmSeg<float> sg{A, B, lda, ldb, k, 0};
+    GemmItem<float, float> it{C, C, ldc, ldc, m, n, 0, 1};
+    StreamScratch scr(sizeof(sg) + sizeof(it) + 64, s);
+    auto *di = static_cast<GemmItem<float, float> *>(scr.p);
+    auto *ds = reinterpret_cast<GemmSeg<float> *>(di + 1);
+    HODLR_CUDA_TRY(cudaMemcpyAsync(di, &it, sizeof(it), cudaMemcpyHostToDevice, s));
+    HODLR_CUDA_TRY(cudaMemcpyAsync(ds, &sg, sizeof(sg), cudaMemcpyHostToDevice, s));
+    if (engine == 1)
+      launch_tc_gemm<float>(di, ds, 1, m, n, transa != 0, alpha, beta, s);
+    else
+      launch_gemm_items<float, float, float>(di, ds, 1, m, n, transa != 0, alpha, beta, s, false);
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    return tc_error_flag(true) > 0 ? HODLR_ERR_TIMEOUT : 0;
   });
 }
 
@@ -509,22 +544,36 @@ int hodlr_init_gaussian(hodlr_system h, unsigned long long seed, double offdiag_
     const long long N = S.N;
     const int m = S.m;
     HODLR_CUDA_TRY(cudaMemsetAsync(S.D.p, 0, sizeof(double) * (size_t)N * S.nmax, s));
+    std::vector<FillTask> fills;
+    long long fmax = 0;
+    auto add_fill = [&](double *a, int rows, int cols, unsigned sid, double sc, double dg) {
+      FillTask f{};
+      f.a = a; f.lda = N; f.rows = rows; f.cols = cols; f.stream_id = sid;
+      f.scale = sc; f.diag_add = dg;
+      fills.push_back(f);
+      fmax = std::max(fmax, (long long)rows * cols);
+    };
     for (size_t q = 0; q < t.leaves.size(); ++q) {
       const Node &n = t.nodes[t.leaves[q]];
-      launch_gauss_fill(S.D.p + n.row_beg, N, n.nrow, n.nrow, seed, (unsigned)(1 + q),
-                        1.0 / std::sqrt((double)n.nrow), 2.0, 0, s);
+      add_fill(S.D.p + n.row_beg, n.nrow, n.nrow, (unsigned)(1 + q),
+               1.0 / std::sqrt((double)n.nrow), 2.0);
     }
     const unsigned base = (unsigned)(1 + t.leaves.size());
     for (size_t i = 1; i < t.nodes.size(); ++i) {
       const Node &c = t.nodes[i];
       const double sc = 1.0 / std::sqrt((double)c.ncol * c.nrow);
-      launch_gauss_fill(S.U.p + c.row_beg + (long long)(c.col_beg - m) * N, N, c.nrow, c.ncol,
-                        seed, base + 2 * (unsigned)i, sc, 0.0, 0, s);
-      launch_gauss_fill(S.V.p + c.row_beg + (long long)(c.col_beg - m) * N, N, c.nrow, c.vncol,
-                        seed, base + 2 * (unsigned)i + 1, sc, 0.0, 0, s);
+      add_fill(S.U.p + c.row_beg + (long long)(c.col_beg - m) * N, c.nrow, c.ncol,
+               base + 2 * (unsigned)i, sc, 0.0);
+      add_fill(S.V.p + c.row_beg + (long long)(c.col_beg - m) * N, c.nrow, c.vncol,
+               base + 2 * (unsigned)i + 1, sc, 0.0);
     }
-    launch_gauss_fill(S.B.p, N, N, m, seed, base + 2 * (unsigned)t.nodes.size() + 2, 1.0, 0.0, 0,
-                      s);
+    add_fill(S.B.p, (int)N, m, base + 2 * (unsigned)t.nodes.size() + 2, 1.0, 0.0);
+    {
+      DevBuf<FillTask> df;
+      df.upload(fills);
+      launch_gauss_fill_batched(df.p, (int)fills.size(), fmax, seed, s);
+      HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    }
     // Rescale each off-diagonal block U_c V_s^T to spectral norm offdiag_norm:
     // ||U V^T||_2^2 = lambda_max((U^T U)(V^T V)); Grams via chunked reduces.
     std::vector<int> ids;
@@ -620,13 +669,26 @@ int hodlr_init_gaussian(hodlr_system h, unsigned long long seed, double offdiag_
     std::vector<double> hf;
     for (size_t i = 1; i < t.nodes.size(); ++i) { hf.push_back(scale_u[i]); hf.push_back(scale_v[i]); }
     fac.upload(hf);
+    std::vector<FillTask> sc;
+    long long smax = 0;
     for (size_t i = 1; i < t.nodes.size(); ++i) {
       const Node &c = t.nodes[i];
-      launch_scale_cols(S.U.p + c.row_beg + (long long)(c.col_beg - m) * N, N, c.nrow, c.ncol,
-                        fac.p + 2 * (i - 1), s);
-      launch_scale_cols(S.V.p + c.row_beg + (long long)(c.col_beg - m) * N, N, c.nrow, c.vncol,
-                        fac.p + 2 * (i - 1) + 1, s);
+      FillTask f{};
+      f.lda = N;
+      f.rows = c.nrow;
+      f.a = S.U.p + c.row_beg + (long long)(c.col_beg - m) * N;
+      f.cols = c.ncol;
+      f.factor = fac.p + 2 * (i - 1);
+      sc.push_back(f);
+      f.a = S.V.p + c.row_beg + (long long)(c.col_beg - m) * N;
+      f.cols = c.vncol;
+      f.factor = fac.p + 2 * (i - 1) + 1;
+      sc.push_back(f);
+      smax = std::max(smax, (long long)c.nrow * std::max(c.ncol, c.vncol));
     }
+    DevBuf<FillTask> dsc;
+    dsc.upload(sc);
+    launch_scale_batched(dsc.p, (int)sc.size(), smax, s);
     HODLR_CUDA_TRY(cudaStreamSynchronize(s));
     S.factored = -1;
     return 0;

@@ -13,8 +13,13 @@
 // Tile 64 x 128 x 16 (64 x 32 x 16 for items of at most 32 columns) per
 // CTA, 256 threads, 4 x 8 (4 x 2) register tile per thread,
 // operands staged through shared memory with a one-tile register prefetch.
+#include <type_traits>
+
+#include <cstdlib>
+
 #include "common.cuh"
 #include "gemm_simt.cuh"
+#include "tc_gemm.cuh"
 
 namespace hodlr {
 
@@ -257,12 +262,157 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tiled items (N > 32): BM x 128 tile per CTA (BM = 64 or 128), 256 threads,
+// TM x 8 register tile per thread (thread x -> rows, y -> columns, so the
+// epilogue's column-major accesses coalesce), K staged in BK-deep slices through a
+// two-stage cp.async pipeline.  Register fragments are interleaved in
+// 16-byte vectors (2 doubles / 4 floats) so that the shared-memory reads of
+// the 16 row groups of a warp are contiguous (no bank conflicts) and the
+// column fragments are warp-broadcasts.
+// ---------------------------------------------------------------------------
+
+__device__ inline void cp_async_elem(void *smem, const void *gmem, int bytes, bool pred) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  const int n = pred ? bytes : 0;
+  if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ inline void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+template <typename T, typename TC, bool TRANS, int BM>
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1)
+    gemm_tile_kernel(const GemmItem<T, TC> *__restrict__ items,
+                     const GemmSeg<T> *__restrict__ segs, T alpha, T beta) {
+  constexpr int BN = 128;
+  constexpr int BK = sizeof(T) == 8 ? 8 : 16;
+  constexpr int VW = 16 / sizeof(T);       // elements per 16-byte vector
+  constexpr int TM = BM / 16, TN = BN / 16;
+  constexpr int AP = BM + 4, BP = BN + 4;  // padded row strides (16-byte multiples)
+  constexpr int NA = BK * BM / NT, NBL = BK * BN / NT;
+  __shared__ __align__(16) T As[2][BK * AP];
+  __shared__ __align__(16) T Bs[2][BK * BP];
+  const GemmItem<T, TC> it = items[blockIdx.x];
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.z * BN;
+  if (m0 >= it.M || n0 >= it.N) return;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
+
+  T acc[TM][TN];
+  // alpha = +-1, beta = 1 (the in-place updates): start from alpha * Cin so the
+  // C loads overlap the main loop; alpha * (alpha * c + s) == c + alpha * s exactly
+  const bool preload = it.Cin && beta == T(1) && (alpha == T(1) || alpha == T(-1));
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      T v = T(0);
+      if (preload) {
+        const int gm = m0 + (i / VW) * (16 * VW) + tx * VW + (i % VW);
+        const int gn = n0 + (j / VW) * (16 * VW) + ty * VW + (j % VW);
+        if (gm < it.M && gn < it.N) v = alpha * T(it.Cin[gm + (long long)gn * it.ldcin]);
+      }
+      acc[i][j] = v;
+    }
+
+  for (int sgi = it.seg_begin; sgi < it.seg_begin + it.seg_count; ++sgi) {
+    const GemmSeg<T> sg = segs[sgi];
+    const int K = sg.K;
+    if (K <= 0) continue;
+    const int ntiles = (K + BK - 1) / BK;
+    auto issue = [&](int kt, int buf) {
+      const int k0 = kt * BK;
+#pragma unroll
+      for (int u = 0; u < NA; ++u) {
+        const int idx = tid + u * NT;
+        int k, m;
+        if (TRANS) { k = idx % BK; m = idx / BK; }
+        else { m = idx % BM; k = idx / BM; }
+        const int gk = k0 + k, gm = m0 + m;
+        const bool ok = gk < K && gm < it.M;
+        const T *src = ok ? (TRANS ? sg.A + gk + (long long)gm * sg.lda
+                                   : sg.A + gm + (long long)gk * sg.lda)
+                          : sg.A;
+        cp_async_elem(&As[buf][k * AP + m], src, sizeof(T), ok);
+      }
+#pragma unroll
+      for (int u = 0; u < NBL; ++u) {
+        const int idx = tid + u * NT;
+        const int k = idx % BK, n = idx / BK;
+        const int gk = k0 + k, gn = n0 + n;
+        const bool ok = gk < K && gn < it.N;
+        const T *src = ok ? sg.B + gk + (long long)gn * sg.ldb : sg.B;
+        cp_async_elem(&Bs[buf][k * BP + n], src, sizeof(T), ok);
+      }
+    };
+    issue(0, 0);
+    cp_async_commit();
+    for (int kt = 0; kt < ntiles; ++kt) {
+      if (kt + 1 < ntiles) issue(kt + 1, (kt + 1) & 1);
+      cp_async_commit();
+      cp_async_wait1();
+      __syncthreads();
+      const T *Ab = As[kt & 1];
+      const T *Bb = Bs[kt & 1];
+      using V = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+#pragma unroll
+      for (int kk = 0; kk < BK; ++kk) {
+        T a[TM], b[TN];
+#pragma unroll
+        for (int g = 0; g < TM / VW; ++g) {
+          const V va = *reinterpret_cast<const V *>(Ab + kk * AP + g * (16 * VW) + tx * VW);
+          const T *pv = reinterpret_cast<const T *>(&va);
+#pragma unroll
+          for (int v = 0; v < VW; ++v) a[g * VW + v] = pv[v];
+        }
+#pragma unroll
+        for (int g = 0; g < TN / VW; ++g) {
+          const V vb = *reinterpret_cast<const V *>(Bb + kk * BP + g * (16 * VW) + ty * VW);
+          const T *pv = reinterpret_cast<const T *>(&vb);
+#pragma unroll
+          for (int v = 0; v < VW; ++v) b[g * VW + v] = pv[v];
+        }
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+          for (int j = 0; j < TN; ++j) acc[i][j] += a[i] * b[j];
+      }
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < TN; ++j) {
+    const int gn = n0 + (j / VW) * (16 * VW) + ty * VW + (j % VW);
+    if (gn >= it.N) continue;
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int gm = m0 + (i / VW) * (16 * VW) + tx * VW + (i % VW);
+      if (gm >= it.M) continue;
+      T v = alpha * acc[i][j];
+      if (it.Cin && !preload) v += beta * T(it.Cin[gm + (long long)gn * it.ldcin]);
+      it.C[gm + (long long)gn * it.ldc] = TC(v);
+    }
+  }
+}
+
 }  // namespace
+
+// FP32 GEMM items (N > 32) run on the tensor cores unless HODLR_TC=0.
+bool tc_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("HODLR_TC");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 
 template <typename TA, typename TC, typename TACC>
 void launch_gemm_items(const GemmItem<TA, TC> *items, const GemmSeg<TA> *segs, int nitems,
                        int max_m, int max_n, bool trans, TACC alpha, TACC beta,
-                       cudaStream_t s) {
+                       cudaStream_t s, bool allow_tc) {
   if (nitems <= 0 || max_m <= 0 || max_n <= 0) return;
   if (max_n <= 32) {
     if (trans) {
@@ -278,6 +428,25 @@ void launch_gemm_items(const GemmItem<TA, TC> *items, const GemmSeg<TA> *segs, i
       else
         skinny_nn_kernel<TA, TC, TACC, 32><<<grid, NT, 0, s>>>(items, segs, alpha, beta);
     }
+  } else if (std::is_same<TA, float>::value && std::is_same<TC, float>::value && allow_tc &&
+             tc_enabled()) {
+    launch_tc_gemm<float>(reinterpret_cast<const GemmItem<float, float> *>(items),
+                          reinterpret_cast<const GemmSeg<float> *>(segs), nitems, max_m, max_n,
+                          trans, float(alpha), float(beta), s);
+    return;
+  } else if (std::is_same<TA, TACC>::value) {
+    using T = TACC;
+    const auto *it2 = reinterpret_cast<const GemmItem<T, TC> *>(items);
+    const auto *sg2 = reinterpret_cast<const GemmSeg<T> *>(segs);
+    if (max_m <= 64) {
+      dim3 grid(nitems, cdiv(max_m, 64), cdiv(max_n, 128));
+      if (trans) gemm_tile_kernel<T, TC, true, 64><<<grid, NT, 0, s>>>(it2, sg2, alpha, beta);
+      else gemm_tile_kernel<T, TC, false, 64><<<grid, NT, 0, s>>>(it2, sg2, alpha, beta);
+    } else {
+      dim3 grid(nitems, cdiv(max_m, 128), cdiv(max_n, 128));
+      if (trans) gemm_tile_kernel<T, TC, true, 128><<<grid, NT, 0, s>>>(it2, sg2, alpha, beta);
+      else gemm_tile_kernel<T, TC, false, 128><<<grid, NT, 0, s>>>(it2, sg2, alpha, beta);
+    }
   } else {
     dim3 grid(nitems, cdiv(max_m, BM), cdiv(max_n, 128));
     if (trans)
@@ -291,12 +460,12 @@ void launch_gemm_items(const GemmItem<TA, TC> *items, const GemmSeg<TA> *segs, i
 template void launch_gemm_items<double, double, double>(const GemmItem<double, double> *,
                                                         const GemmSeg<double> *, int, int,
                                                         int, bool, double, double,
-                                                        cudaStream_t);
+                                                        cudaStream_t, bool);
 template void launch_gemm_items<float, double, double>(const GemmItem<float, double> *,
                                                        const GemmSeg<float> *, int, int, int,
-                                                       bool, double, double, cudaStream_t);
+                                                       bool, double, double, cudaStream_t, bool);
 template void launch_gemm_items<float, float, float>(const GemmItem<float, float> *,
                                                      const GemmSeg<float> *, int, int, int,
-                                                     bool, float, float, cudaStream_t);
+                                                     bool, float, float, cudaStream_t, bool);
 
 }  // namespace hodlr

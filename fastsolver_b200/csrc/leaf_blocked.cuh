@@ -1,0 +1,43 @@
+// leaf_blocked.cuh -- batched blocked factorization of the leaves on [D | X].
+#pragma once
+#include "common.cuh"
+
+namespace hodlr {
+
+// Panel width: the panel (n x NB) lives in shared memory, so it narrows for
+// leaves above 512 rows (the library accepts leaves of up to 1024 rows).
+template <typename T>
+inline int leaf_nb(int max_n) {
+  if (sizeof(T) == 8) return max_n <= 512 ? 32 : 16;
+  return max_n <= 512 ? 64 : 32;
+}
+
+// One leaf of a batched factorization.
+template <typename T>
+struct LeafFactorTask {
+  T *D;            // n x n, ldd: LU factors on output (LAPACK layout)
+  T *X;            // n x ncols, ldx: D^{-1} X on output
+  int *ipiv;       // n: LAPACK pivots
+  int *perm;       // n: final row order
+  T *Linv;         // npanels x NB x NB: inverses of the unit-lower diagonal blocks
+  T *Uinv;         // npanels x NB x NB: inverses of the upper diagonal blocks
+  int *swapflag;   // npanels: panel had row interchanges
+  long long ldd;
+  long long ldx;
+  int n;
+  int ncols;
+  int info_slot;
+  int pad;
+};
+
+template <typename T>
+void launch_leaf_init(const LeafFactorTask<T> *tasks, int count, int *info, cudaStream_t s);
+template <typename T>
+void launch_leaf_panel(const LeafFactorTask<T> *tasks, int count, int max_n, int nb, int k0,
+                       int panel, int *info, cudaStream_t s);
+// max_cols: largest n + ncols over the leaves
+template <typename T>
+void launch_leaf_laswp(const LeafFactorTask<T> *tasks, int count, int max_cols, int nb, int k0,
+                       int panel, cudaStream_t s);
+
+}  // namespace hodlr

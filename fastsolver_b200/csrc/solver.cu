@@ -21,6 +21,7 @@
 
 #include "gemm_simt.cuh"
 #include "leaf.cuh"
+#include "leaf_blocked.cuh"
 #include "node.cuh"
 #include "solver.h"
 
@@ -78,6 +79,123 @@ void path_need(const Tree &t, bool factor, int chunk, size_t &part, size_t &wfin
   }
 }
 
+
+// Per-panel GEMM item lists of the blocked leaf factorization (see
+// leaf_blocked.cu): forward steps on [D | X], then the backward solve on X.
+template <typename T>
+void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long ldx,
+                     int *ipiv, int *perm, bool factor_cols_all, int m, LeafPlan<T> &lp) {
+  const int nleaf = (int)t.leaves.size();
+  int max_panels = 0;
+  lp.max_n = 0;
+  for (int id : t.leaves) lp.max_n = std::max(lp.max_n, t.nodes[id].nrow);
+  const int NB = leaf_nb<T>(lp.max_n);
+  lp.nb = NB;
+  for (int id : t.leaves) max_panels = std::max(max_panels, cdiv(t.nodes[id].nrow, NB));
+  lp.Linv.ensure((size_t)nleaf * max_panels * NB * NB);
+  lp.Uinv.ensure((size_t)nleaf * max_panels * NB * NB);
+  lp.swapflag.ensure((size_t)nleaf * max_panels);
+  std::vector<LeafFactorTask<T>> tasks(nleaf);
+  lp.laswp_cols = 0;
+  for (int q = 0; q < nleaf; ++q) {
+    const Node &nd = t.nodes[t.leaves[q]];
+    LeafFactorTask<T> &k = tasks[q];
+    k.D = Dbase + nd.row_beg;
+    k.ldd = ldd;
+    k.X = Xbase + nd.row_beg;
+    k.ldx = ldx;
+    k.ipiv = ipiv + nd.row_beg;
+    k.perm = perm + nd.row_beg;
+    k.Linv = lp.Linv.p + (size_t)q * max_panels * NB * NB;
+    k.Uinv = lp.Uinv.p + (size_t)q * max_panels * NB * NB;
+    k.swapflag = lp.swapflag.p + (size_t)q * max_panels;
+    k.n = nd.nrow;
+    k.ncols = factor_cols_all ? nd.col_beg + nd.ncol : m;
+    k.info_slot = q;
+    lp.laswp_cols = std::max(lp.laswp_cols, k.n + k.ncols);
+  }
+  lp.tasks.upload(tasks);
+  lp.nleaf = nleaf;
+  lp.fwd.clear();
+  lp.bwd.clear();
+  for (int pi = 0; pi < max_panels; ++pi) {
+    const int k0 = pi * NB;
+    auto F = std::make_unique<typename LeafPlan<T>::Fwd>();
+    F->k0 = k0;
+    F->panel = pi;
+    std::vector<GemmItem<T, T>> ti, ui;
+    std::vector<GemmSeg<T>> ts, us;
+    for (int q = 0; q < nleaf; ++q) {
+      const LeafFactorTask<T> &k = tasks[q];
+      if (k0 >= k.n) continue;
+      const int kb = std::min(NB, k.n - k0);
+      const int rest = k.n - k0 - kb;
+      const T *Li = k.Linv + (size_t)pi * NB * NB;
+      // U12 = L11^{-1} A12 in place: D columns right of the panel, X columns
+      auto trsm = [&](T *C, long long ldc, int N) {
+        if (N <= 0) return;
+        GemmSeg<T> g{Li, C, NB, ldc, kb, 0};
+        GemmItem<T, T> it{C, nullptr, ldc, 0, kb, N, (int)ts.size(), 1};
+        ts.push_back(g);
+        ti.push_back(it);
+      };
+      trsm(k.D + k0 + (long long)(k0 + kb) * ldd, ldd, rest);
+      trsm(k.X + k0, ldx, k.ncols);
+      if (rest > 0) {
+        const T *L21 = k.D + (k0 + kb) + (long long)k0 * ldd;
+        auto upd = [&](T *C, long long ldc, const T *B, long long ldb, int N) {
+          if (N <= 0) return;
+          GemmSeg<T> g{L21, B, ldd, ldb, kb, 0};
+          GemmItem<T, T> it{C, C, ldc, ldc, rest, N, (int)us.size(), 1};
+          us.push_back(g);
+          ui.push_back(it);
+        };
+        upd(k.D + (k0 + kb) + (long long)(k0 + kb) * ldd, ldd,
+            k.D + k0 + (long long)(k0 + kb) * ldd, ldd, rest);
+        upd(k.X + (k0 + kb), ldx, k.X + k0, ldx, k.ncols);
+      }
+    }
+    F->trsm.set(ti, ts);
+    F->update.set(ui, us);
+    lp.fwd.push_back(std::move(F));
+  }
+  for (int pi = max_panels - 1; pi >= 0; --pi) {
+    const int k0 = pi * NB;
+    auto B = std::make_unique<typename LeafPlan<T>::Bwd>();
+    std::vector<GemmItem<T, T>> ti, ui;
+    std::vector<GemmSeg<T>> ts, us;
+    for (int q = 0; q < nleaf; ++q) {
+      const LeafFactorTask<T> &k = tasks[q];
+      if (k0 >= k.n || k.ncols <= 0) continue;
+      const int kb = std::min(NB, k.n - k0);
+      const T *Ui = k.Uinv + (size_t)pi * NB * NB;
+      T *Xk = k.X + k0;
+      GemmSeg<T> g{Ui, Xk, NB, ldx, kb, 0};
+      GemmItem<T, T> it{Xk, nullptr, ldx, 0, kb, k.ncols, (int)ts.size(), 1};
+      ts.push_back(g);
+      ti.push_back(it);
+      if (k0 > 0) {
+        GemmSeg<T> g2{k.D + (long long)k0 * ldd, Xk, ldd, ldx, kb, 0};
+        GemmItem<T, T> it2{k.X, k.X, ldx, ldx, k0, k.ncols, (int)us.size(), 1};
+        us.push_back(g2);
+        ui.push_back(it2);
+      }
+    }
+    B->trsm.set(ti, ts);
+    B->update.set(ui, us);
+    lp.bwd.push_back(std::move(B));
+  }
+}
+
+template <typename TA, typename TC, typename TACC>
+void run_gemm(const GemmLaunch<TA, TC> &g, bool trans, TACC alpha, TACC beta, cudaStream_t s) {
+  launch_gemm_items<TA, TC, TACC>(g.items.p, g.segs.p, g.n, g.max_m, g.max_n, trans, alpha, beta,
+                                  s);
+}
+
+template <typename T>
+void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t s);
+
 template <typename T, typename TE>
 void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan, int form) {
   plan.levels.clear();
@@ -103,6 +221,8 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
   }
   plan.nleaf = (int)lt.size();
   plan.leaf_tasks.upload(lt);
+  if (sp.factor)
+    build_leaf_plan<T>(t, sp.D, sp.ldd, sp.X, sp.ldx, sp.ipiv, sp.perm, true, m, plan.leaf);
   const int nleaf = (int)t.leaves.size();
 
   for (int d = t.max_depth - 1; d >= 0; --d) {
@@ -272,14 +392,33 @@ struct PhaseScope {
   }
 };
 
+template <typename T>
+void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t s) {
+  {
+    PhaseScope ps(pf, PH_GETRF, s);
+    launch_leaf_init<T>(lp.tasks.p, lp.nleaf, info, s);
+    for (const auto &F : lp.fwd) {
+      launch_leaf_panel<T>(lp.tasks.p, lp.nleaf, lp.max_n, lp.nb, F->k0, F->panel, info, s);
+      launch_leaf_laswp<T>(lp.tasks.p, lp.nleaf, lp.laswp_cols, lp.nb, F->k0, F->panel, s);
+      run_gemm<T, T, T>(F->trsm, false, T(1), T(0), s);
+      run_gemm<T, T, T>(F->update, false, T(-1), T(1), s);
+    }
+  }
+  {
+    PhaseScope ps(pf, PH_GETRS, s);
+    for (const auto &B : lp.bwd) {
+      run_gemm<T, T, T>(B->trsm, false, T(1), T(0), s);
+      run_gemm<T, T, T>(B->update, false, T(-1), T(1), s);
+    }
+  }
+}
+
 template <typename T, typename TE>
 void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cudaStream_t s) {
   LeafTask<T> none{};
   if (plan.factor) {
-    PhaseScope ps(pf, PH_GETRF, s);
-    launch_getrf<T>(plan.leaf_tasks.p, none, plan.nleaf, plan.max_n, info, s);
-  }
-  {
+    run_leaf_plan<T>(pf, plan.leaf, info, s);
+  } else {
     PhaseScope ps(pf, PH_GETRS, s);
     launch_getrs<T>(plan.leaf_tasks.p, none, plan.nleaf, plan.max_n, plan.max_nrhs, s);
   }

@@ -8,6 +8,7 @@
 
 #include "common.cuh"
 #include "htree.h"
+#include "leaf_blocked.cuh"
 #include "util.cuh"
 
 namespace hodlr {
@@ -73,12 +74,49 @@ struct LevelPlan {
   int n_bc = 0, bc_max_m = 0, bc_max_n = 0;
 };
 
+// One batched GEMM launch: items + their segments.
+template <typename TA, typename TC>
+struct GemmLaunch {
+  DevBuf<GemmItem<TA, TC>> items;
+  DevBuf<GemmSeg<TA>> segs;
+  int n = 0, max_m = 0, max_n = 0;
+  void set(const std::vector<GemmItem<TA, TC>> &it, const std::vector<GemmSeg<TA>> &sg) {
+    items.upload(it);
+    segs.upload(sg);
+    n = (int)it.size();
+    max_m = max_n = 0;
+    for (const auto &x : it) {
+      max_m = max_m > x.M ? max_m : x.M;
+      max_n = max_n > x.N ? max_n : x.N;
+    }
+  }
+};
+
+// Blocked factorization of every leaf on [D | X] (leaf_blocked.cu).
+template <typename T>
+struct LeafPlan {
+  DevBuf<LeafFactorTask<T>> tasks;
+  DevBuf<T> Linv, Uinv;
+  DevBuf<int> swapflag;
+  int nleaf = 0, max_n = 0, laswp_cols = 0, nb = 0;
+  struct Fwd {
+    int k0, panel;
+    GemmLaunch<T, T> trsm, update;
+  };
+  struct Bwd {
+    GemmLaunch<T, T> trsm, update;
+  };
+  std::vector<std::unique_ptr<Fwd>> fwd;
+  std::vector<std::unique_ptr<Bwd>> bwd;
+};
+
 template <typename T, typename TE>
 struct PathPlan {
   bool built = false;
   bool factor = false;  // getrf + node factor (fused) vs getrs + node apply only
   DevBuf<LeafTask<T>> leaf_tasks;
   int nleaf = 0, max_n = 0, max_nrhs = 0;
+  LeafPlan<T> leaf;     // factor paths: the blocked leaf factorization
   std::vector<std::unique_ptr<LevelPlan<T, TE>>> levels;  // deepest first
 };
 

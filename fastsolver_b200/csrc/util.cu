@@ -185,7 +185,61 @@ __global__ void gauss_fill_kernel(double *a, long long lda, long long rows, long
   }
 }
 
+__global__ void gauss_fill_batched_kernel(const FillTask *__restrict__ tasks,
+                                          unsigned long long seed) {
+  const FillTask tk = tasks[blockIdx.y];
+  const long long rows = tk.rows, total = rows * tk.cols;
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+  for (long long e2 = blockIdx.x * (long long)blockDim.x + threadIdx.x; 2 * e2 < total;
+       e2 += (long long)gridDim.x * blockDim.x) {
+    const uint4 ctr = make_uint4((uint32_t)e2, (uint32_t)(e2 >> 32), tk.stream_id, 0x5eedu);
+    const uint4 rv = philox4x32_10(ctr, key);
+    const double u1 = u53(rv.x, rv.y), u2 = u53(rv.z, rv.w);
+    const double rad = sqrt(-2.0 * log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    const double g[2] = {rad * cs, rad * sn};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long long e = 2 * e2 + h;
+      if (e >= total) break;
+      const long long i = e % rows, j = e / rows;
+      double v = tk.scale * g[h];
+      if (i == j) v += tk.diag_add;
+      tk.a[i + j * tk.lda] = v;
+    }
+  }
+}
+
+__global__ void scale_batched_kernel(const FillTask *__restrict__ tasks) {
+  const FillTask tk = tasks[blockIdx.y];
+  const long long rows = tk.rows, total = rows * tk.cols;
+  const double f = *tk.factor;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e % rows, j = e / rows;
+    tk.a[i + j * tk.lda] *= f;
+  }
+}
+
 }  // namespace
+
+void launch_gauss_fill_batched(const FillTask *tasks, int ntasks, long long max_elems,
+                               unsigned long long seed, cudaStream_t s) {
+  if (ntasks <= 0 || max_elems <= 0) return;
+  const long long b = std::min<long long>(cdiv<long long>((max_elems + 1) / 2, kThreads), 1024);
+  dim3 grid((unsigned)b, ntasks);
+  gauss_fill_batched_kernel<<<grid, kThreads, 0, s>>>(tasks, seed);
+  HODLR_LAUNCH_CHECK();
+}
+
+void launch_scale_batched(const FillTask *tasks, int ntasks, long long max_elems, cudaStream_t s) {
+  if (ntasks <= 0 || max_elems <= 0) return;
+  const long long b = std::min<long long>(cdiv<long long>(max_elems, kThreads), 1024);
+  dim3 grid((unsigned)b, ntasks);
+  scale_batched_kernel<<<grid, kThreads, 0, s>>>(tasks);
+  HODLR_LAUNCH_CHECK();
+}
 
 template <typename TS, typename TD>
 void launch_convert2d(const TS *src, long long lds, TD *dst, long long ldd, long long rows,

@@ -40,4 +40,19 @@ void launch_gauss_fill(double *a, long long lda, long long rows, long long cols,
                        unsigned long long seed, unsigned int stream_id, double scale,
                        double diag_add, long long diag_row0, cudaStream_t s);
 
+// One block of a batched fill / scale: a(i, j), i < rows, j < cols.
+struct FillTask {
+  double *a;
+  long long lda;
+  int rows, cols;
+  unsigned int stream_id;
+  int pad;
+  double scale;     // fill: N(0,1) * scale; scale task: factor index below
+  double diag_add;  // fill: added on i == j
+  const double *factor;  // scale task: a *= *factor
+};
+void launch_gauss_fill_batched(const FillTask *tasks, int ntasks, long long max_elems,
+                               unsigned long long seed, cudaStream_t s);
+void launch_scale_batched(const FillTask *tasks, int ntasks, long long max_elems, cudaStream_t s);
+
 }  // namespace hodlr

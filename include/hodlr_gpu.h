@@ -133,6 +133,15 @@ int hodlr_leaf_solve_batched(int count, const hodlr_leaf_desc *descs,
                              int max_n, int max_nrhs, int *info,
                              hodlr_stream_t stream);
 
+/* FP32 GEMM engine of the mixed-precision path (no reference counterpart):
+ * C = beta * C + alpha * op(A) * B, column-major, op(A) = A (transa = 0,
+ * A m x k) or A^T (transa = 1, A k x m), B k x n.  engine 0: FP32 FMA pipe;
+ * engine 1: tcgen05 tensor cores, split-BF16 (hi*hi + hi*lo + lo*hi, FP32
+ * accumulate; relative error ~2^-16 of |A||B|).  Synchronous. */
+int hodlr_gemm_f32(int transa, int m, int n, int k, float alpha, const float *A,
+                   int lda, const float *B, int ldb, float beta, float *C,
+                   int ldc, int engine, hodlr_stream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* Handle API: the solver that walks the tree (FastSolver + HodlrMatrix)     */
 /* ------------------------------------------------------------------------ */
