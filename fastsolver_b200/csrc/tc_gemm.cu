@@ -27,6 +27,8 @@
 // waits (bounded) for its own MMAs, frees its TMEM and returns.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "tc_gemm.cuh"
 
@@ -36,10 +38,8 @@ __device__ int g_tc_error = 0;
 
 namespace {
 
-constexpr int kThreads = 128;
 constexpr int BM = 128;    // UMMA M
 constexpr int BK = 32;     // K per stage (two MMA k-steps of 16)
-constexpr int STAGES = 3;
 constexpr long long kSpinLimit = 1LL << 26;
 
 __device__ inline uint32_t smem_u32(const void *p) {
@@ -138,212 +138,338 @@ __device__ inline void split_store8(const float *v, unsigned char *hi, unsigned 
   *reinterpret_cast<uint4 *>(lo + off) = *reinterpret_cast<const uint4 *>(l);
 }
 
-// Loads BK K-values of one row of an operand into registers (zero padded).
-// kcontig: element (row, k) at base[k + row * ld] (K contiguous), else at
-// base[row + k * ld] (row contiguous).
-__device__ inline void load_row(float (&v)[BK], const float *base, long long ld, bool kcontig,
-                                int row, int rows_valid, int k0, int K) {
-  if (row >= rows_valid) {
-#pragma unroll
-    for (int k = 0; k < BK; ++k) v[k] = 0.f;
-    return;
-  }
+__device__ inline void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Persistent, warp-specialized split-BF16 GEMM.
+//   warps 0-3 (producers): thread p owns row p of the A tile and of the B
+//     tile.  It stages its rows' FP32 values with asynchronous cp.async
+//     copies kStg stages ahead into its own 128-byte slot of a staging ring
+//     (so a per-thread cp.async.wait_group suffices), then splits the landed
+//     stage into bf16 hi / lo and writes the UMMA K-major ring (full[s]:
+//     128 arrivals, empty[s]: tcgen05.commit).
+//   warp 4 lane 0 (MMA issuer): 3 MMAs per 16-deep k-step into one of two TMEM
+//     accumulators (tfull[a]: commit, tempty[a]: 128 epilogue arrivals).
+//   warps 5-8 (epilogue): thread r owns row r of the tile; it prefetches the
+//     next tile's C row with cp.async as soon as the current tile is drained,
+//     then drains TMEM 16 columns at a time: D = alpha * acc + beta * Cin.
+constexpr int kWarps = 9;
+constexpr int kThreadsP = kWarps * 32;
+constexpr int kStagesP = 2;  // UMMA operand ring
+constexpr int kStg = 3;      // FP32 staging ring (stages in flight per producer)
+
+__device__ inline void cpa4(void *dst, const void *src, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(ok ? 4 : 0));
+}
+__device__ inline void cpa16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src));
+}
+__device__ inline void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ inline void cpa_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Position in the flattened (tile, segment, k0) sequence of a CTA.
+template <typename TC>
+struct KPos {
+  int t, seg, k0;
+  int m0, n0, Mu, Nu;
+  GemmItem<float, TC> it;
+  GemmSeg<float> sg;
+  bool valid;
+};
+
+// Stage one row's BK values of an operand into `dst` (BK floats, the
+// thread's own staging row) with cp.async; zero-filled outside the matrix.
+// The row's eight 16-byte chunks are XOR-swizzled by `sw` (= row & 7) so that
+// the 32 lanes reading their rows chunk by chunk hit distinct banks.
+__device__ inline void stage_row(float *dst, int sw, const float *base, long long ld,
+                                 bool kcontig, int row, int rows_valid, int k0, int K) {
+  auto slot = [&](int k) { return dst + ((((k >> 2) ^ sw) << 2) | (k & 3)); };
   if (kcontig) {
     const float *p = base + (long long)row * ld + k0;
-    const bool full = (k0 + BK <= K) && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);
-    if (full) {
+    const bool inrow = row < rows_valid;
+    if (inrow && k0 + BK <= K && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
 #pragma unroll
-      for (int q = 0; q < BK / 4; ++q) {
-        const float4 x = __ldg(reinterpret_cast<const float4 *>(p) + q);
-        v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
-      }
+      for (int q = 0; q < BK / 4; ++q) cpa16(slot(4 * q), p + 4 * q);
     } else {
 #pragma unroll
-      for (int k = 0; k < BK; ++k) v[k] = (k0 + k < K) ? __ldg(p + k) : 0.f;
+      for (int k = 0; k < BK; ++k) {
+        const bool ok = inrow && k0 + k < K;
+        cpa4(slot(k), ok ? p + k : base, ok);
+      }
     }
   } else {
+    const bool inrow = row < rows_valid;
     const float *p = base + row + (long long)k0 * ld;
 #pragma unroll
-    for (int k = 0; k < BK; ++k) v[k] = (k0 + k < K) ? __ldg(p + (long long)k * ld) : 0.f;
+    for (int k = 0; k < BK; ++k) {
+      const bool ok = inrow && k0 + k < K;
+      cpa4(slot(k), ok ? p + (long long)k * ld : base, ok);
+    }
   }
 }
 
 template <int BN, typename TC>
-__global__ void __launch_bounds__(kThreads)
-    tc_gemm_kernel(const GemmItem<float, TC> *__restrict__ items,
-                   const GemmSeg<float> *__restrict__ segs, float alpha, float beta, int trans,
-                   int swap) {
+__global__ void __launch_bounds__(kThreadsP, 1)
+    tc_gemm_persistent(const GemmItem<float, TC> *__restrict__ items,
+                       const GemmSeg<float> *__restrict__ segs, int nitems, int mtiles,
+                       int ntn, float alpha, float beta, int trans, int swap) {
   constexpr int A_BYTES = BM * BK * 2;  // one of hi / lo
   constexpr int B_BYTES = BN * BK * 2;
   constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-  constexpr int BROWS = BN / kThreads > 0 ? BN / kThreads : 1;  // B rows per thread
+  constexpr int STG_BYTES = 2 * 128 * BK * 4;  // A and B rows of the 128 producers
+  constexpr int TMEM_COLS = 2 * BN;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar_empty[STAGES];
-  __shared__ __align__(8) uint64_t bar_done;
-  __shared__ uint32_t tmem_base_sh;
-  __shared__ int abort_sh;
-
-  const GemmItem<float, TC> it = items[blockIdx.x];
-  // UMMA-M side (rows of D) and UMMA-N side (columns of D)
-  const int Mu = swap ? it.N : it.M;
-  const int Nu = swap ? it.M : it.N;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.z * BN;
-  if (m0 >= Mu || n0 >= Nu) return;
+  unsigned char *ring = smem;
+  float *stg = reinterpret_cast<float *>(smem + kStagesP * STAGE_BYTES);
+  float *cst = stg + kStg * (STG_BYTES / 4);  // C tile staging, BN x 128
+  __shared__ __align__(8) uint64_t full[kStagesP], empty[kStagesP], tfull[2], tempty[2], fin;
+  __shared__ uint32_t tmem_sh;
+  __shared__ volatile int abort_sh;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int total = nitems * mtiles * ntn;
 
   if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) mbar_init(&bar_empty[s], 1);
-    mbar_init(&bar_done, 1);
+    for (int s = 0; s < kStagesP; ++s) {
+      mbar_init(&full[s], 128);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 128);
+    }
+    mbar_init(&fin, 1);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  constexpr int TMEM_COLS = BN < 32 ? 32 : BN;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
-                     smem_u32(&tmem_base_sh)),
+                     smem_u32(&tmem_sh)),
                  "r"(TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = tmem_base_sh;
-  const uint32_t idesc = instr_desc(BM, BN);
+  const uint32_t tmem = tmem_sh;
 
-  // total K tiles over all segments
-  int ntiles = 0;
-  for (int s = it.seg_begin; s < it.seg_begin + it.seg_count; ++s)
-    ntiles += (segs[s].K + BK - 1) / BK;
-
-  // operand access for the current tile: the UMMA A operand has rows along
-  // Mu, the UMMA B operand rows along Nu
-  int seg = it.seg_begin, seg_k0 = 0;
-  GemmSeg<float> sg = segs[seg];
-  while (seg < it.seg_begin + it.seg_count - 1 && sg.K <= 0) sg = segs[++seg];
-  auto advance = [&]() {
-    seg_k0 += BK;
-    while (seg < it.seg_begin + it.seg_count - 1 && seg_k0 >= sg.K) {
-      ++seg;
-      seg_k0 = 0;
-      sg = segs[seg];
-    }
+  auto decode = [&](int t, GemmItem<float, TC> &it, int &m0, int &n0, int &Mu, int &Nu) {
+    const int item = t / (mtiles * ntn);
+    const int rem = t - item * (mtiles * ntn);
+    m0 = (rem / ntn) * BM;
+    n0 = (rem % ntn) * BN;
+    it = items[item];
+    Mu = swap ? it.N : it.M;
+    Nu = swap ? it.M : it.N;
+    return m0 < Mu && n0 < Nu;
   };
-  // item operand A (op(A): M x K) and B (K x N); element access helpers
-  // UMMA-A rows = item rows (M) unless swapped (then item columns N).
-  float va[BK], vb[BROWS][BK];
-  auto fetch = [&]() {
-    const int K = sg.K;
-    if (!swap) {
-      // UMMA A = op(A): row m; trans: A[k + m*lda] (K contiguous), else A[m + k*lda]
-      load_row(va, sg.A, sg.lda, trans != 0, m0 + tid, it.M, seg_k0, K);
-#pragma unroll
-      for (int r = 0; r < BROWS; ++r) {
-        const int n = n0 + tid + r * kThreads;
-        load_row(vb[r], sg.B, sg.ldb, true, n, (tid + r * kThreads < BN) ? it.N : -1, seg_k0, K);
-      }
-    } else {
-      // D^T = B^T op(A)^T: UMMA A row = item column n of B (K contiguous),
-      // UMMA B row = item row m of op(A) (trans: K contiguous)
-      load_row(va, sg.B, sg.ldb, true, m0 + tid, it.N, seg_k0, K);
-#pragma unroll
-      for (int r = 0; r < BROWS; ++r) {
-        const int m = n0 + tid + r * kThreads;
-        load_row(vb[r], sg.A, sg.lda, trans != 0, m, (tid + r * kThreads < BN) ? it.M : -1,
-                 seg_k0, K);
+  auto kstages = [&](const GemmItem<float, TC> &it) {
+    int n = 0;
+    for (int s = it.seg_begin; s < it.seg_begin + it.seg_count; ++s) n += (segs[s].K + BK - 1) / BK;
+    return n;
+  };
+  // first / next k-stage of the CTA's flattened sequence (skips empty tiles
+  // and zero-length segments)
+  auto first_in_tile = [&](KPos<TC> &ps) {
+    for (; ps.t < total; ps.t += gridDim.x) {
+      if (!decode(ps.t, ps.it, ps.m0, ps.n0, ps.Mu, ps.Nu)) continue;
+      for (ps.seg = ps.it.seg_begin; ps.seg < ps.it.seg_begin + ps.it.seg_count; ++ps.seg) {
+        ps.sg = segs[ps.seg];
+        if (ps.sg.K > 0) { ps.k0 = 0; ps.valid = true; return; }
       }
     }
+    ps.valid = false;
+  };
+  auto next = [&](KPos<TC> &ps) {
+    ps.k0 += BK;
+    if (ps.k0 < ps.sg.K) return;
+    for (++ps.seg; ps.seg < ps.it.seg_begin + ps.it.seg_count; ++ps.seg) {
+      ps.sg = segs[ps.seg];
+      if (ps.sg.K > 0) { ps.k0 = 0; return; }
+    }
+    ps.t += gridDim.x;
+    first_in_tile(ps);
   };
 
-  bool ok = true;
-  bool committed_done = false;
-  if (ntiles > 0) fetch();
-  for (int kt = 0; kt < ntiles; ++kt) {
-    const int st = kt % STAGES;
-    unsigned char *base = smem + st * STAGE_BYTES;
-    unsigned char *ahi = base, *alo = base + A_BYTES;
-    unsigned char *bhi = base + 2 * A_BYTES, *blo = bhi + B_BYTES;
-    if (kt >= STAGES) {
-      if (!mbar_wait(&bar_empty[st], ((kt / STAGES) - 1) & 1)) ok = false;
-    }
-    if (!ok) atomicExch(&abort_sh, 1);
-    // convert + store this thread's rows
-#pragma unroll
-    for (int c = 0; c < BK / 8; ++c) split_store8(va + 8 * c, ahi, alo, kmajor_off(BM, tid, c));
-#pragma unroll
-    for (int r = 0; r < BROWS; ++r) {
-      const int row = tid + r * kThreads;
-      if (row < BN)
-#pragma unroll
-        for (int c = 0; c < BK / 8; ++c)
-          split_store8(vb[r] + 8 * c, bhi, blo, kmajor_off(BN, row, c));
-    }
-    fence_proxy_async();
-    tc_fence_before();
-    __syncthreads();
-    if (abort_sh) break;
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t a_hi = smem_u32(ahi), a_lo = smem_u32(alo);
-      const uint32_t b_hi = smem_u32(bhi), b_lo = smem_u32(blo);
-#pragma unroll
-      for (int ks = 0; ks < BK / 16; ++ks) {
-        const uint32_t ao = ks * (BM / 8) * 256, bo = ks * (BN / 8) * 256;
-        const uint64_t dah = smem_desc(a_hi + ao, 128, 256), dal = smem_desc(a_lo + ao, 128, 256);
-        const uint64_t dbh = smem_desc(b_hi + bo, 128, 256), dbl = smem_desc(b_lo + bo, 128, 256);
-        const uint32_t acc0 = (kt > 0 || ks > 0) ? 1u : 0u;
-        mma_bf16(tmem, dah, dbh, idesc, acc0);
-        mma_bf16(tmem, dah, dbl, idesc, 1u);
-        mma_bf16(tmem, dal, dbh, idesc, 1u);
+  if (warp < 4) {
+    // ------------------------------------------------------------ producers
+    const int p = tid;
+    KPos<TC> iss, con;
+    iss.t = con.t = blockIdx.x;
+    first_in_tile(iss);
+    first_in_tile(con);
+    auto issue = [&](KPos<TC> &ps, int slot) {
+      float *a = stg + slot * (STG_BYTES / 4) + p * BK;
+      float *b = a + 128 * BK;
+      if (ps.valid) {
+        const GemmSeg<float> &sg = ps.sg;
+        const int sw = p & 7;
+        if (!swap) {
+          stage_row(a, sw, sg.A, sg.lda, trans != 0, ps.m0 + p, ps.it.M, ps.k0, sg.K);
+          stage_row(b, sw, sg.B, sg.ldb, true, ps.n0 + p, p < BN ? ps.it.N : -1, ps.k0, sg.K);
+        } else {
+          stage_row(a, sw, sg.B, sg.ldb, true, ps.m0 + p, ps.it.N, ps.k0, sg.K);
+          stage_row(b, sw, sg.A, sg.lda, trans != 0, ps.n0 + p, p < BN ? ps.it.M : -1, ps.k0,
+                    sg.K);
+        }
+        next(ps);
       }
-      mma_commit(&bar_empty[st]);
-      if (kt == ntiles - 1) mma_commit(&bar_done);
+      cpa_commit();
+    };
+    int islot = 0;
+    for (int i = 0; i < kStg - 1; ++i) { issue(iss, islot); islot = (islot + 1) % kStg; }
+    int stage = 0, cslot = 0;
+    uint32_t phase = 0;
+    while (con.valid && !abort_sh) {
+      issue(iss, islot);
+      islot = (islot + 1) % kStg;
+      cpa_wait<kStg - 1>();  // this thread's copies of stage `cslot` have landed
+      const float *a = stg + cslot * (STG_BYTES / 4) + p * BK;
+      const float *b = a + 128 * BK;
+      float va[BK], vb[BK];
+#pragma unroll
+      for (int q = 0; q < BK / 4; ++q) {
+        const int qs = q ^ (p & 7);
+        const float4 x = reinterpret_cast<const float4 *>(a)[qs];
+        const float4 y = reinterpret_cast<const float4 *>(b)[qs];
+        va[4 * q] = x.x; va[4 * q + 1] = x.y; va[4 * q + 2] = x.z; va[4 * q + 3] = x.w;
+        vb[4 * q] = y.x; vb[4 * q + 1] = y.y; vb[4 * q + 2] = y.z; vb[4 * q + 3] = y.w;
+      }
+      cslot = (cslot + 1) % kStg;
+      if (!mbar_wait(&empty[stage], phase ^ 1)) { abort_sh = 1; break; }
+      unsigned char *base = ring + stage * STAGE_BYTES;
+      unsigned char *ahi = base, *alo = base + A_BYTES;
+      unsigned char *bhi = base + 2 * A_BYTES, *blo = bhi + B_BYTES;
+#pragma unroll
+      for (int c = 0; c < BK / 8; ++c) split_store8(va + 8 * c, ahi, alo, kmajor_off(BM, p, c));
+      if (p < BN) {
+#pragma unroll
+        for (int c = 0; c < BK / 8; ++c) split_store8(vb + 8 * c, bhi, blo, kmajor_off(BN, p, c));
+      }
+      fence_proxy_async();
+      mbar_arrive(&full[stage]);
+      if (++stage == kStagesP) { stage = 0; phase ^= 1; }
+      next(con);
     }
-    if (kt == ntiles - 1) committed_done = true;
-    if (kt + 1 < ntiles) {
-      advance();
-      fetch();
+    cpa_wait<0>();
+  } else if (warp == 4) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = instr_desc(BM, BN);
+      int stage = 0, acc = 0;
+      uint32_t phase = 0, aphase = 0;
+      for (int t = blockIdx.x; t < total && !abort_sh; t += gridDim.x) {
+        GemmItem<float, TC> it;
+        int m0, n0, Mu, Nu;
+        if (!decode(t, it, m0, n0, Mu, Nu)) continue;
+        if (!mbar_wait(&tempty[acc], aphase ^ 1)) { abort_sh = 1; break; }
+        tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(acc * BN);
+        const int nst = kstages(it);
+        for (int ks_all = 0; ks_all < nst; ++ks_all) {
+          if (!mbar_wait(&full[stage], phase)) { abort_sh = 1; break; }
+          tc_fence_after();
+          const uint32_t a_hi = smem_u32(ring + stage * STAGE_BYTES), a_lo = a_hi + A_BYTES;
+          const uint32_t b_hi = a_hi + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
+#pragma unroll
+          for (int ks = 0; ks < BK / 16; ++ks) {
+            const uint32_t ao = ks * (BM / 8) * 256, bo = ks * (BN / 8) * 256;
+            const uint64_t dah = smem_desc(a_hi + ao, 128, 256), dal = smem_desc(a_lo + ao, 128, 256);
+            const uint64_t dbh = smem_desc(b_hi + bo, 128, 256), dbl = smem_desc(b_lo + bo, 128, 256);
+            mma_bf16(d, dah, dbh, idesc, (ks_all > 0 || ks > 0) ? 1u : 0u);
+            mma_bf16(d, dah, dbl, idesc, 1u);
+            mma_bf16(d, dal, dbh, idesc, 1u);
+          }
+          mma_commit(&empty[stage]);
+          if (++stage == kStagesP) { stage = 0; phase ^= 1; }
+        }
+        if (abort_sh) break;
+        mma_commit(&tfull[acc]);
+        if (++acc == 2) { acc = 0; aphase ^= 1; }
+      }
+      mma_commit(&fin);  // all MMAs of this CTA complete before TMEM is freed
+      if (!mbar_wait(&fin, 0)) abort_sh = 1;
     }
-  }
-  if (ntiles > 0 && !committed_done) {
-    // aborted: track this CTA's issued MMAs on bar_done before freeing TMEM
-    if (tid == 0) mma_commit(&bar_done);
-    committed_done = true;
-  }
-  bool done_ok = true;
-  if (ntiles > 0) done_ok = mbar_wait(&bar_done, 0);
-  if (!ok || !done_ok || abort_sh) {
-    if (tid == 0) atomicExch(&g_tc_error, 1);
   } else {
-    tc_fence_after();
-    // epilogue: warp w owns D rows 32w .. 32w + 31 (TMEM lanes)
-    const int drow = m0 + warp * 32 + lane;
-#pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 16) {
-      uint32_t r[16];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
-          "%10, %11, %12, %13, %14, %15}, [%16];\n"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-            "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-            "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      if (drow < Mu) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int dcol = n0 + c0 + j;
-          if (dcol >= Nu) break;
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;        // TMEM lane quarter of this warp
+    const int rl = q * 32 + lane;  // row of the tile owned by this thread
+    int acc = 0;
+    uint32_t aphase = 0;
+    // C staging [col][128 rows]: each thread copies and reads only its row
+    auto issue_c = [&](const GemmItem<float, TC> &it, int m0, int n0, int Mu, int Nu) {
+      const int drow = m0 + rl;
+      if (it.Cin != nullptr && sizeof(TC) == 4) {
+        const float *cin = reinterpret_cast<const float *>(it.Cin);
+        for (int j = 0; j < BN; ++j) {
+          const int dcol = n0 + j;
+          const bool ok = drow < Mu && dcol < Nu;
           const int gm = swap ? dcol : drow, gn = swap ? drow : dcol;
-          float v = ntiles > 0 ? alpha * __uint_as_float(r[j]) : 0.f;
-          if (it.Cin) v += beta * float(it.Cin[gm + (long long)gn * it.ldcin]);
-          it.C[gm + (long long)gn * it.ldc] = TC(v);
+          cpa4(cst + j * 128 + rl, ok ? cin + gm + (long long)gn * it.ldcin : cin, ok);
         }
       }
+      cpa_commit();
+    };
+    int t = blockIdx.x;
+    GemmItem<float, TC> it;
+    int m0 = 0, n0 = 0, Mu = 0, Nu = 0;
+    auto next_tile = [&]() {
+      for (; t < total; t += gridDim.x)
+        if (decode(t, it, m0, n0, Mu, Nu)) return true;
+      return false;
+    };
+    bool have = next_tile();
+    if (have) issue_c(it, m0, n0, Mu, Nu);
+    while (have && !abort_sh) {
+      const bool has_k = kstages(it) > 0;
+      const int drow = m0 + rl;
+      if (!mbar_wait(&tfull[acc], aphase)) { abort_sh = 1; break; }
+      tc_fence_after();
+      cpa_wait<0>();  // this tile's C rows have landed
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN && n0 + c0 < Nu; c0 += 16) {
+        uint32_t r[16];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+            "%10, %11, %12, %13, %14, %15}, [%16];\n"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+              "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+              "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (drow < Mu) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int dcol = n0 + c0 + j;
+            if (dcol >= Nu) break;
+            const int gm = swap ? dcol : drow, gn = swap ? drow : dcol;
+            float v = has_k ? alpha * __uint_as_float(r[j]) : 0.f;
+            if (it.Cin) {
+              const float c = sizeof(TC) == 4 ? cst[(c0 + j) * 128 + rl]
+                                              : float(it.Cin[gm + (long long)gn * it.ldcin]);
+              v += beta * c;
+            }
+            it.C[gm + (long long)gn * it.ldc] = TC(v);
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&tempty[acc]);
+      if (++acc == 2) { acc = 0; aphase ^= 1; }
+      t += gridDim.x;
+      have = next_tile();
+      if (have) issue_c(it, m0, n0, Mu, Nu);  // lands while the next tile is computed
     }
+    cpa_wait<0>();
   }
   tc_fence_before();
   __syncthreads();
+  if (abort_sh && tid == 0) atomicExch(&g_tc_error, 1);
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
                  "r"(TMEM_COLS));
@@ -354,12 +480,23 @@ void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int
                int mu_max, int nu_max, bool trans, bool swap, float alpha, float beta,
                cudaStream_t s) {
   constexpr int STAGE_BYTES = 2 * BM * BK * 2 + 2 * BN * BK * 2;
-  const size_t smem = (size_t)STAGES * STAGE_BYTES + 128;
-  HODLR_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<BN, TC>,
+  constexpr int STG_BYTES = 2 * 128 * BK * 4;
+  const size_t smem =
+      (size_t)kStagesP * STAGE_BYTES + (size_t)kStg * STG_BYTES + (size_t)BN * 128 * 4 + 128;
+  HODLR_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_persistent<BN, TC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid(nitems, cdiv(mu_max, BM), cdiv(nu_max, BN));
-  tc_gemm_kernel<BN, TC><<<grid, kThreads, smem, s>>>(items, segs, alpha, beta, trans ? 1 : 0,
-                                                      swap ? 1 : 0);
+  const int mt = cdiv(mu_max, BM), nt = cdiv(nu_max, BN);
+  const long long total = (long long)nitems * mt * nt;
+  int sms = 148;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+  }
+  const int grid = (int)std::min<long long>(total, sms);
+  tc_gemm_persistent<BN, TC><<<grid, kThreadsP, smem, s>>>(items, segs, nitems, mt, nt, alpha,
+                                                           beta, trans ? 1 : 0, swap ? 1 : 0);
   HODLR_LAUNCH_CHECK();
 }
 
