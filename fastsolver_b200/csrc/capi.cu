@@ -270,54 +270,67 @@ static int node_solve_common(int form, int r0, int r1, int c, const double *V0Tu
   if (int e = device_ok()) return e;
   return guarded([&]() -> int {
     cudaStream_t s = as_stream(stream);
-    // scratch: task | S (s x s) | S^{-1} (s x s) | I (s x s) | VTu0 | VTu1 | piv | info
-    //          | gram item + segment
-    const size_t nS = (size_t)s_ * s_;
-    const size_t need = 256 + sizeof(double) * (3 * nS + 2 * (size_t)r0 * r1) +
-                        sizeof(int) * (s_ + 8) + 512;
+    // scratch: task | S (r0 x r0) | F (r1 x r0) | I (r0 x r0) | M (s2 x s2) | eta (s2 x c)
+    //          | info | gram item + segment | apply item + 2 segments
+    const int s2 = r0 + r1;
+    const size_t nR = (size_t)r0 * r0, nF = (size_t)r1 * r0, nM = (size_t)s2 * s2;
+    const size_t nE = (size_t)s2 * (c > 0 ? c : 1);
+    const size_t need = 256 + sizeof(double) * (2 * nR + nF + nM + nE) + 8 * sizeof(int) + 1024;
     StreamScratch scr(need, s);
     char *base = static_cast<char *>(scr.p);
     auto *task = reinterpret_cast<NodeTask<double, double> *>(base);
-    double *S_lu = reinterpret_cast<double *>(base + 256);
-    double *S_inv = S_lu + nS;
-    double *ident = S_inv + nS;
-    double *VTu0 = ident + nS;
-    double *VTu1 = VTu0 + (size_t)r0 * r1;
-    int *piv = reinterpret_cast<int *>(VTu1 + (size_t)r0 * r1);
-    int *info_dev = info ? info : piv + s_;
+    double *S = reinterpret_cast<double *>(base + 256);
+    double *F = S + nR;
+    double *ident = F + nF;
+    double *M = ident + nR;
+    double *eta = M + nM;
+    int *info_dev = reinterpret_cast<int *>(eta + nE);
     auto *gitem = reinterpret_cast<GemmItem<double, double> *>(
-        (reinterpret_cast<uintptr_t>(piv + s_ + 8) + 15) & ~uintptr_t(15));
+        (reinterpret_cast<uintptr_t>(info_dev + 8) + 15) & ~uintptr_t(15));
     auto *gseg = reinterpret_cast<GemmSeg<double> *>(gitem + 1);
+    auto *aitem = reinterpret_cast<GemmItem<double, double> *>(gseg + 1);
+    auto *aseg = reinterpret_cast<GemmSeg<double> *>(aitem + 1);
     NodeTask<double, double> k{};
-    k.W0d = V0Td0; k.W0u = V0Tu0; k.W1d = V1Td1; k.W1u = V1Tu1;
-    k.w0_stride = k.w1_stride = 0;
-    k.ldw0d = ld0d; k.ldw0u = ld00; k.ldw1d = ld1d; k.ldw1u = ld11;
-    k.np0 = k.np1 = 1;
-    k.r0 = r0; k.r1 = r1; k.c = c;
-    // outputs in place: form 0 writes eta0 over V1Td1, eta1 over V0Td0
-    // (fast_solver.cc:238-240); form 1 eta0 over V0Td0, eta1 over V1Td1.
-    if (form == 0) { k.eta0 = V1Td1; k.ld_eta0 = ld1d; k.eta1 = V0Td0; k.ld_eta1 = ld0d; }
-    else { k.eta0 = V0Td0; k.ld_eta0 = ld0d; k.eta1 = V1Td1; k.ld_eta1 = ld1d; }
-    k.S_lu = S_lu; k.S_inv = S_inv; k.S_piv = piv; k.VTu0 = VTu0; k.VTu1 = VTu1;
-    k.info_slot = 0;
+    k.W0u = V0Tu0; k.W1u = V1Tu1; k.ldw0u = ld00; k.ldw1u = ld11;
+    k.S = S; k.F = F; k.M = M;
+    k.r0 = r0; k.r1 = r1; k.info_slot = 0;
     HODLR_CUDA_TRY(cudaMemcpyAsync(task, &k, sizeof(k), cudaMemcpyHostToDevice, s));
+    std::vector<double> I(nR, 0.0);
+    for (int i = 0; i < r0; ++i) I[(size_t)i * r0 + i] = 1.0;
+    GemmSeg<double> g{V1Tu1, V0Tu0, ld11, ld00, r1, 0};
+    GemmItem<double, double> git{S, ident, r0, r0, r0, r0, 0, 1};
+    GemmSeg<double> a2[2] = {{M, V0Td0, s2, ld0d, r1, 0},
+                             {M + (size_t)r1 * s2, V1Td1, s2, ld1d, r0, 0}};
+    GemmItem<double, double> ait{eta, nullptr, s2, 0, s2, c, 0, 2};
     if (form == 0) {
-      // S = I - V1Tu1 V0Tu0 into S_lu (the dgemm at solver_tasks.cc:261)
-      std::vector<double> I(nS, 0.0);
-      for (int i = 0; i < s_; ++i) I[(size_t)i * s_ + i] = 1.0;
-      HODLR_CUDA_TRY(cudaMemcpyAsync(ident, I.data(), sizeof(double) * nS, cudaMemcpyHostToDevice, s));
-      GemmSeg<double> g{V1Tu1, V0Tu0, ld11, ld00, r1, 0};
-      GemmItem<double, double> it{S_lu, ident, r0, s_, r0, r0, 0, 1};
-      HODLR_CUDA_TRY(cudaMemcpyAsync(gitem, &it, sizeof(it), cudaMemcpyHostToDevice, s));
+      // S = I - V1Tu1 V0Tu0 (the dgemm at solver_tasks.cc:261)
+      HODLR_CUDA_TRY(cudaMemcpyAsync(ident, I.data(), sizeof(double) * nR, cudaMemcpyHostToDevice, s));
+      HODLR_CUDA_TRY(cudaMemcpyAsync(gitem, &git, sizeof(git), cudaMemcpyHostToDevice, s));
       HODLR_CUDA_TRY(cudaMemcpyAsync(gseg, &g, sizeof(g), cudaMemcpyHostToDevice, s));
       launch_gemm_items<double, double, double>(gitem, gseg, 1, r0, r0, false, -1.0, 1.0, s);
-      HODLR_CUDA_TRY(cudaStreamSynchronize(s));  // host staging buffers go out of scope
     }
-    launch_node_factor<double, double>(task, 1, s_, form, info_dev, s);
-    if (c > 0) launch_node_apply<double, double>(task, 1, s_, r0 + r1, c, form, s);
-    int rc = finish_info(info, info_dev, s);
-    if (info) HODLR_CUDA_TRY(cudaStreamSynchronize(s));  // scratch lifetime
-    return rc;
+    HODLR_CUDA_TRY(cudaMemcpyAsync(aitem, &ait, sizeof(ait), cudaMemcpyHostToDevice, s));
+    HODLR_CUDA_TRY(cudaMemcpyAsync(aseg, a2, sizeof(a2), cudaMemcpyHostToDevice, s));
+    launch_node_factor<double, double>(task, 1, form == 0 ? r0 : s2, r0 > r1 ? r0 : r1, form,
+                                       info_dev, s);
+    int hinfo = 0;
+    HODLR_CUDA_TRY(cudaMemcpyAsync(&hinfo, info_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));  // also ends the host staging buffers' use
+    if (info) HODLR_CUDA_TRY(cudaMemcpyAsync(info, info_dev, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    if (hinfo == 0 && c > 0) {
+      launch_gemm_items<double, double, double>(aitem, aseg, 1, s2, c, false, 1.0, 0.0, s);
+      // outputs in place: form 0 writes eta0 over V1Td1, eta1 over V0Td0
+      // (fast_solver.cc:238-240); form 1 eta0 over V0Td0, eta1 over V1Td1.
+      double *o0 = form == 0 ? V1Td1 : V0Td0;
+      double *o1 = form == 0 ? V0Td0 : V1Td1;
+      const int l0 = form == 0 ? ld1d : ld0d, l1 = form == 0 ? ld0d : ld1d;
+      HODLR_CUDA_TRY(cudaMemcpy2DAsync(o0, sizeof(double) * l0, eta, sizeof(double) * s2,
+                                       sizeof(double) * r0, c, cudaMemcpyDeviceToDevice, s));
+      HODLR_CUDA_TRY(cudaMemcpy2DAsync(o1, sizeof(double) * l1, eta + r0, sizeof(double) * s2,
+                                       sizeof(double) * r1, c, cudaMemcpyDeviceToDevice, s));
+    }
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));  // scratch lifetime
+    return info ? 0 : hinfo;  // with a device INFO pointer the value goes there
   });
 }
 

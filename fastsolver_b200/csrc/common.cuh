@@ -104,22 +104,21 @@ struct GemmItem {
 // order.  `form` (a launch argument) 0 is LUSolveTask's r x r reduced system
 // (solver_tasks.cc:139-305), 1 the 2r x 2r permuted Schur system of the
 // leaf-internal branch (solver_tasks.cc:483-535).
+// One node of a level's capacitance factorization.  With the children's
+// reduce results W0 = V0^T [d0 | u0] and W1 = V1^T [d1 | u1], the factor
+// kernel writes the node's solve matrix M ((r0 + r1) x (r1 + r0), ld r0 + r1)
+// such that [eta0; eta1] = M [V0Td0; V1Td1].
 template <typename TW, typename TE>
 struct NodeTask {
-  const TW *W0d, *W0u, *W1d, *W1u;
-  long long w0_stride, w1_stride;
-  long long ldw0d, ldw0u, ldw1d, ldw1u;
-  TE *eta0;           // r0 x c out, ld ld_eta0: broadcast into child 0
-  TE *eta1;           // r1 x c out, ld ld_eta1: broadcast into child 1
-  long long ld_eta0, ld_eta1;
-  double *S_lu;       // s x s: S before factoring (form 0), then its LU
-  int *S_piv;         // s, 0-based pivot rows
-  double *S_inv;      // s x s: S^{-1} from the LU factors
-  double *VTu0;       // r1 x r0: V0^T u0 (factor writes, apply reads)
-  double *VTu1;       // r0 x r1: V1^T u1
-  int np0, np1;
-  int r0, r1, c;
+  const TW *W0u;      // V0^T u0: r1 x r0, ld ldw0u
+  const TW *W1u;      // V1^T u1: r0 x r1, ld ldw1u
+  long long ldw0u, ldw1u;
+  const double *S;    // form 0: S = I - V1Tu1 V0Tu0 (r0 x r0, ld r0), FP64
+  double *F;          // form 0: r1 x r0 FP64 work (-V0Tu0 S^{-1})
+  TE *M;              // out: (r0 + r1)^2, ld r0 + r1
+  int r0, r1;
   int info_slot;
+  int pad;
 };
 
 }  // namespace hodlr

@@ -19,6 +19,7 @@
 
 #include "common.cuh"
 #include "gemm_simt.cuh"
+#include "gemm_skinny.cuh"
 #include "tc_gemm.cuh"
 
 namespace hodlr {
@@ -414,6 +415,13 @@ void launch_gemm_items(const GemmItem<TA, TC> *items, const GemmSeg<TA> *segs, i
                        int max_m, int max_n, bool trans, TACC alpha, TACC beta,
                        cudaStream_t s, bool allow_tc) {
   if (nitems <= 0 || max_m <= 0 || max_n <= 0) return;
+  if (max_n <= 32 && std::is_same<TA, TC>::value && std::is_same<TA, TACC>::value) {
+    using T = TACC;
+    launch_skinny<T>(reinterpret_cast<const GemmItem<T, T> *>(items),
+                     reinterpret_cast<const GemmSeg<T> *>(segs), nitems, max_m, max_n, trans,
+                     alpha, beta, s);
+    return;
+  }
   if (max_n <= 32) {
     if (trans) {
       dim3 grid(nitems, cdiv(max_m, 64), cdiv(max_n, 16));

@@ -30,6 +30,18 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// 16-byte vector of T
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using V = float4;
+};
+template <>
+struct Vec16<double> {
+  using V = double2;
+};
+
 template <typename T>
 __device__ inline T tabs(T v) {
   return v < T(0) ? -v : v;
@@ -210,6 +222,271 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Register-resident panel LU, same semantics as leaf_panel_kernel (LAPACK
+// dgetf2 pivot order, implicit interchanges, inverses of the diagonal block).
+// 512 threads; thread t owns panel rows t + 512 q (q < RPT) in registers, so
+// an elimination step touches no shared memory except the pivot row.  Per
+// column: every warp finds its best candidate (largest |a|, lowest current
+// position on ties) and the winning lane publishes its whole row; one
+// barrier; every warp combines the candidates with four shuffles, reads the
+// pivot row (broadcast) and eliminates its rows.  The loop over the NB
+// columns is unrolled so that the row lives in registers.
+constexpr int kRegThreads = 512;
+
+// Warp-wide argmax of |a| with the lowest position on ties (idamax order),
+// with warp reductions on the bit patterns (|a| >= 0 orders like its bits).
+// In: per lane (best = |a| or anything when pos == INT_MAX, pos, code).
+// Out: every lane holds the winner's (best, pos, code) and its lane index;
+// pos == INT_MAX when no lane had a candidate.
+__device__ inline void warp_argmax(float &best, int &pos, int &code, int &wlane) {
+  const bool cand = pos != 0x7fffffff;
+  const unsigned key = cand ? __float_as_uint(best) : 0u;
+  const unsigned mx = __reduce_max_sync(0xffffffffu, key);
+  const unsigned pm = __reduce_min_sync(0xffffffffu, key == mx ? (unsigned)pos : 0xffffffffu);
+  const unsigned win = __ballot_sync(0xffffffffu, cand && key == mx && (unsigned)pos == pm);
+  wlane = win ? __ffs(win) - 1 : 0;
+  best = __uint_as_float(mx);
+  pos = win ? (int)pm : 0x7fffffff;
+  code = __shfl_sync(0xffffffffu, code, wlane);
+  if (!win) code = -1;
+}
+__device__ inline void warp_argmax(double &best, int &pos, int &code, int &wlane) {
+  const bool cand = pos != 0x7fffffff;
+  const unsigned long long b = cand ? (unsigned long long)__double_as_longlong(best) : 0ull;
+  const unsigned hi = (unsigned)(b >> 32), lo = (unsigned)b;
+  const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+  const bool top = hi == mh && lo == ml;
+  const unsigned pm = __reduce_min_sync(0xffffffffu, top ? (unsigned)pos : 0xffffffffu);
+  const unsigned win = __ballot_sync(0xffffffffu, cand && top && (unsigned)pos == pm);
+  wlane = win ? __ffs(win) - 1 : 0;
+  best = __longlong_as_double((long long)(((unsigned long long)mh << 32) | ml));
+  pos = win ? (int)pm : 0x7fffffff;
+  code = __shfl_sync(0xffffffffu, code, wlane);
+  if (!win) code = -1;
+}
+
+template <typename T, int NB, int RPT>
+__global__ void __launch_bounds__(kRegThreads, 1)
+    leaf_panel_reg_kernel(const LeafFactorTask<T> *__restrict__ tasks, int k0, int panel,
+                          int *info) {
+  constexpr int NW = kRegThreads / 32;
+  constexpr int LDL = NB + 1;
+  constexpr int VW = 16 / sizeof(T);
+  using V = typename Vec16<T>::V;
+  __shared__ __align__(16) T wrow[2][NW][NB];
+  __shared__ T wval[2][NW];
+  __shared__ int wpos[2][NW], wcode[2][NW];
+  __shared__ T Lr[NB * LDL], Ur[NB * LDL];
+  __shared__ T udr[NB];
+  __shared__ int pv[NB];
+  const LeafFactorTask<T> tk = tasks[blockIdx.x];
+  const int n = tk.n;
+  if (k0 >= n) return;
+  const int kb = min(NB, n - k0);
+  const int R = n - k0;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  T *D = tk.D;
+  const long long ldd = tk.ldd;
+  T a[RPT][NB];
+  int pos[RPT];
+  bool live[RPT];
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    const int i = tid + q * kRegThreads;
+    live[q] = i < R;
+    pos[q] = i;
+    const T *src = D + (k0 + i) + (long long)k0 * ldd;
+#pragma unroll
+    for (int c = 0; c < NB; ++c) a[q][c] = (live[q] && c < kb) ? src[(long long)c * ldd] : T(0);
+  }
+  bool warp_live = __any_sync(0xffffffffu, live[0]);
+  int info_local = 0;
+  bool swaps = false;
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+    if (j >= kb) break;
+    const int slot = j & 1;
+    if (warp_live) {
+      T best = T(0);
+      int bp = 0x7fffffff, bc = -1;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        if (live[q] && pos[q] >= j) {
+          const T av = tabs(a[q][j]);
+          // NaN is never a candidate (as idamax, which skips it)
+          if (av == av && (bp == 0x7fffffff || av > best || (av == best && pos[q] < bp))) {
+            best = av; bp = pos[q]; bc = tid + q * kRegThreads;
+          }
+        }
+      }
+      int wl;
+      warp_argmax(best, bp, bc, wl);
+      // the winning lane publishes its row
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        if (bc >= 0 && bc == tid + q * kRegThreads) {
+          V *dst = reinterpret_cast<V *>(wrow[slot][warp]);
+#pragma unroll
+          for (int cv = 0; cv < NB / VW; ++cv) {
+            V v;
+            T *vp = reinterpret_cast<T *>(&v);
+#pragma unroll
+            for (int u = 0; u < VW; ++u) vp[u] = a[q][cv * VW + u];
+            dst[cv] = v;
+          }
+        }
+      }
+      if (lane == 0) { wval[slot][warp] = best; wpos[slot][warp] = bp; wcode[slot][warp] = bc; }
+    } else if (lane == 0) {
+      wval[slot][warp] = T(0); wpos[slot][warp] = 0x7fffffff; wcode[slot][warp] = -1;
+    }
+    __syncthreads();
+    // combine the warp candidates (every thread, same result)
+    T pb = T(0);
+    int pp = 0x7fffffff, pc = -1, pw = 0;
+    if (lane < NW) { pb = wval[slot][lane]; pp = wpos[slot][lane]; pc = wcode[slot][lane]; }
+    warp_argmax(pb, pp, pc, pw);  // pw: the winning warp
+    int p = j;
+    T piv = T(0);
+    if (pc >= 0) { p = pp; piv = wrow[slot][pw][j]; }
+    if (tid == 0) pv[j] = p;
+    if (p != j) swaps = true;
+    if (warp_live) {
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        if (live[q]) {
+          if (tid + q * kRegThreads == pc) pos[q] = j;
+          else if (pos[q] == j) pos[q] = p;
+        }
+      }
+      if (piv != T(0)) {
+        const T rinv = sizeof(T) == 4 ? T(__frcp_rn(float(piv))) : T(__drcp_rn(double(piv)));
+        const V *prow = reinterpret_cast<const V *>(wrow[slot][pw]);
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          if (live[q] && pos[q] > j) {
+            const T l = a[q][j] * rinv;
+            a[q][j] = l;
+#pragma unroll
+            for (int cv = (j + 1) / VW; cv < NB / VW; ++cv) {
+              const V v = prow[cv];
+              const T *vp = reinterpret_cast<const T *>(&v);
+#pragma unroll
+              for (int u = 0; u < VW; ++u)
+                if (cv * VW + u > j) a[q][cv * VW + u] -= l * vp[u];
+            }
+          }
+        }
+      }
+    }
+    if (piv == T(0) && info_local == 0) info_local = k0 + j + 1;
+  }
+  // rows to their final positions; diagonal block rows to shared memory
+  int pold[RPT];
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    pold[q] = live[q] ? tk.perm[k0 + tid + q * kRegThreads] : 0;
+    if (live[q]) {
+      T *dst = D + (k0 + pos[q]) + (long long)k0 * ldd;
+#pragma unroll
+      for (int c = 0; c < NB; ++c)
+        if (c < kb) dst[(long long)c * ldd] = a[q][c];
+      if (pos[q] < kb) {
+        const int r = pos[q];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+          Lr[r * LDL + c] = c < r ? a[q][c] : (c == r ? T(1) : T(0));
+          Ur[r * LDL + c] = c >= r ? a[q][c] : T(0);
+        }
+      }
+    }
+  }
+  for (int r = kb + tid; r < NB; r += kRegThreads) {
+    for (int c = 0; c < NB; ++c) {
+      Lr[r * LDL + c] = c == r ? T(1) : T(0);
+      Ur[r * LDL + c] = c == r ? T(1) : T(0);
+    }
+  }
+  __syncthreads();  // every thread has read its perm entry and written its rows
+#pragma unroll
+  for (int q = 0; q < RPT; ++q)
+    if (live[q]) tk.perm[k0 + pos[q]] = pold[q];
+  for (int j = tid; j < kb; j += kRegThreads) tk.ipiv[k0 + j] = k0 + pv[j] + 1;
+  for (int r = tid; r < NB; r += kRegThreads) udr[r] = T(1) / Ur[r * LDL + r];
+  if (tid == 0) {
+    tk.swapflag[panel] = swaps ? 1 : 0;
+    if (info_local && info && info[tk.info_slot] == 0) info[tk.info_slot] = info_local;
+  }
+  __syncthreads();
+  // inverses of the diagonal block, four columns per warp pass: lanes hold
+  // rows lane + 32 r of the columns; x_k is broadcast with a shuffle
+  constexpr int RPL = (NB + 31) / 32;
+  T *Lout = tk.Linv + (size_t)panel * NB * NB;
+  T *Uout = tk.Uinv + (size_t)panel * NB * NB;
+  for (int j0 = warp * 4; j0 < NB; j0 += NW * 4) {
+    T x[4][RPL];
+    // L^{-1}: forward substitution on e_j
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc)
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) x[cc][r] = (lane + 32 * r == j0 + cc) ? T(1) : T(0);
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+      T xk[4];
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) xk[cc] = __shfl_sync(0xffffffffu, x[cc][k / 32], k % 32);
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        if (i > k && i < NB) {
+          const T l = Lr[i * LDL + k];
+#pragma unroll
+          for (int cc = 0; cc < 4; ++cc) x[cc][r] -= l * xk[cc];
+        }
+      }
+    }
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc)
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        if (i < NB && j0 + cc < NB) Lout[i + (j0 + cc) * NB] = x[cc][r];
+      }
+    // U^{-1}: back substitution on e_j
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc)
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) x[cc][r] = (lane + 32 * r == j0 + cc) ? T(1) : T(0);
+#pragma unroll
+    for (int k = NB - 1; k >= 0; --k) {
+      T xk[4];
+      const T dk = udr[k];
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        xk[cc] = __shfl_sync(0xffffffffu, x[cc][k / 32], k % 32) * dk;
+        if (lane == k % 32) x[cc][k / 32] = xk[cc];
+      }
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        if (i < k) {
+          const T u = Ur[i * LDL + k];
+#pragma unroll
+          for (int cc = 0; cc < 4; ++cc) x[cc][r] -= u * xk[cc];
+        }
+      }
+    }
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc)
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        if (i < NB && j0 + cc < NB) Uout[i + (j0 + cc) * NB] = x[cc][r];
+      }
+  }
+}
+
 // Row interchanges of panel `panel` on every column of D outside the panel
 // and on the leaf's X columns.  grid (column block, leaf); thread = column.
 template <typename T>
@@ -247,6 +524,157 @@ __global__ void leaf_init_kernel(const LeafFactorTask<T> *__restrict__ tasks, in
   if (threadIdx.x == 0 && info) info[tk.info_slot] = 0;
 }
 
+// ---- apply: X <- U^{-1} L^{-1} P X with the stored blocked factors.
+//
+// One CTA per (column chunk of MC right-hand sides, leaf).  The chunk of P X
+// lives in shared memory (row-major, padded rows); per panel the diagonal
+// block is applied with its explicit inverse and the rest of the block
+// column of L (forward) or U (backward) is streamed from global memory once,
+// coalesced along the rows, into register accumulators.  Every element of the
+// factors is read once per chunk.
+constexpr int kApplyThreads = 512;
+
+
+// y (kb x MC in shared memory, row stride XS) <- Ainv (kb x kb, column-major, ld nb) y.
+// Ainv is first copied to shared memory `As` (kb x kb, ld kb + 1) with every
+// load independent, so the product runs from shared memory.
+template <typename T, int MC, int XS>
+__device__ inline void apply_diag(const T *__restrict__ Ainv, int nb, T *y, int kb, T *As) {
+  constexpr int VW = 16 / sizeof(T);
+  constexpr int NV = MC / VW;
+  constexpr int OUT = (64 * NV + kApplyThreads - 1) / kApplyThreads;
+  using V = typename Vec16<T>::V;
+  const int tid = threadIdx.x;
+  const int lds = kb + 1;
+  for (int e = tid; e < kb * kb; e += kApplyThreads) {
+    const int i = e % kb, k = e / kb;
+    As[i + k * lds] = Ainv[i + (size_t)k * nb];
+  }
+  __syncthreads();
+  T acc[OUT][VW];
+#pragma unroll
+  for (int o = 0; o < OUT; ++o) {
+#pragma unroll
+    for (int v = 0; v < VW; ++v) acc[o][v] = T(0);
+    const int e = tid + o * kApplyThreads;
+    if (e < kb * NV) {
+      const int i = e % kb, jv = e / kb;
+#pragma unroll 8
+      for (int k = 0; k < kb; ++k) {
+        const T a = As[i + k * lds];
+        const V x = *reinterpret_cast<const V *>(y + k * XS + jv * VW);
+        const T *xp = reinterpret_cast<const T *>(&x);
+#pragma unroll
+        for (int v = 0; v < VW; ++v) acc[o][v] += a * xp[v];
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int o = 0; o < OUT; ++o) {
+    const int e = tid + o * kApplyThreads;
+    if (e < kb * NV) {
+      const int i = e % kb, jv = e / kb;
+      V out;
+      T *op = reinterpret_cast<T *>(&out);
+#pragma unroll
+      for (int v = 0; v < VW; ++v) op[v] = acc[o][v];
+      *reinterpret_cast<V *>(y + i * XS + jv * VW) = out;
+    }
+  }
+  __syncthreads();
+}
+
+// dst (rows x MC, shared, stride XS) -= A (rows x kb, global, ld lda) y (kb x MC, shared)
+template <typename T, int MC, int XS>
+__device__ inline void apply_block(const T *__restrict__ A, long long lda, T *dst, int rows,
+                                   const T *y, int kb) {
+  constexpr int VW = 16 / sizeof(T);
+  using V = typename Vec16<T>::V;
+  for (int i = threadIdx.x; i < rows; i += kApplyThreads) {
+    T acc[MC];
+#pragma unroll
+    for (int j = 0; j < MC; j += VW) {
+      const V x = *reinterpret_cast<const V *>(dst + i * XS + j);
+      const T *xp = reinterpret_cast<const T *>(&x);
+#pragma unroll
+      for (int v = 0; v < VW; ++v) acc[j + v] = xp[v];
+    }
+    const T *Ai = A + i;
+    int k = 0;
+    for (; k + 16 <= kb; k += 16) {
+      T a[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) a[u] = Ai[(long long)(k + u) * lda];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const T *yk = y + (k + u) * XS;
+#pragma unroll
+        for (int j = 0; j < MC; j += VW) {
+          const V x = *reinterpret_cast<const V *>(yk + j);
+          const T *xp = reinterpret_cast<const T *>(&x);
+#pragma unroll
+          for (int v = 0; v < VW; ++v) acc[j + v] -= a[u] * xp[v];
+        }
+      }
+    }
+    for (; k < kb; ++k) {
+      const T a = Ai[(long long)k * lda];
+      const T *yk = y + k * XS;
+#pragma unroll
+      for (int j = 0; j < MC; ++j) acc[j] -= a * yk[j];
+    }
+#pragma unroll
+    for (int j = 0; j < MC; j += VW) {
+      V out;
+      T *op = reinterpret_cast<T *>(&out);
+#pragma unroll
+      for (int v = 0; v < VW; ++v) op[v] = acc[j + v];
+      *reinterpret_cast<V *>(dst + i * XS + j) = out;
+    }
+  }
+}
+
+template <typename T, int MC>
+__global__ void __launch_bounds__(kApplyThreads)
+    leaf_apply_kernel(const LeafFactorTask<T> *__restrict__ tasks, int nb, int max_n) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int XS = MC + 16 / sizeof(T);  // padded row stride (16 bytes)
+  const LeafFactorTask<T> tk = tasks[blockIdx.y];
+  const int n = tk.n;
+  const int c0 = blockIdx.x * MC;
+  if (c0 >= tk.ncols || n <= 0) return;
+  const int mc = min(MC, tk.ncols - c0);
+  const int tid = threadIdx.x;
+  T *xs = reinterpret_cast<T *>(smem_raw);
+  T *As = xs + (size_t)max_n * XS;  // diagonal inverse, nb x (nb + 1)
+  T *X = tk.X + (long long)c0 * tk.ldx;
+  const long long ldx = tk.ldx, ldd = tk.ldd;
+  for (int e = tid; e < n * MC; e += kApplyThreads) {
+    const int i = e % n, j = e / n;
+    xs[i * XS + j] = j < mc ? X[tk.perm[i] + (long long)j * ldx] : T(0);
+  }
+  __syncthreads();
+  const int np = (n + nb - 1) / nb;
+  for (int p = 0; p < np; ++p) {
+    const int k0 = p * nb, kb = min(nb, n - k0);
+    apply_diag<T, MC, XS>(tk.Linv + (size_t)p * nb * nb, nb, xs + k0 * XS, kb, As);
+    apply_block<T, MC, XS>(tk.D + (k0 + kb) + (long long)k0 * ldd, ldd, xs + (k0 + kb) * XS,
+                           n - k0 - kb, xs + k0 * XS, kb);
+    __syncthreads();
+  }
+  for (int p = np - 1; p >= 0; --p) {
+    const int k0 = p * nb, kb = min(nb, n - k0);
+    apply_diag<T, MC, XS>(tk.Uinv + (size_t)p * nb * nb, nb, xs + k0 * XS, kb, As);
+    apply_block<T, MC, XS>(tk.D + (long long)k0 * ldd, ldd, xs, k0, xs + k0 * XS, kb);
+    __syncthreads();
+  }
+  for (int e = tid; e < n * mc; e += kApplyThreads) {
+    const int i = e % n, j = e / n;
+    X[i + (long long)j * ldx] = xs[i * XS + j];
+  }
+}
+
 }  // namespace
 
 template <int NB, typename T>
@@ -275,10 +703,30 @@ void launch_leaf_panel_nb(const LeafFactorTask<T> *tasks, int count, int max_n, 
   HODLR_LAUNCH_CHECK();
 }
 
+template <typename T, int NB, int RPT>
+void launch_leaf_panel_reg(const LeafFactorTask<T> *tasks, int count, int k0, int panel,
+                           int *info, cudaStream_t s) {
+  leaf_panel_reg_kernel<T, NB, RPT><<<count, kRegThreads, 0, s>>>(tasks, k0, panel, info);
+  HODLR_LAUNCH_CHECK();
+}
+
 template <typename T>
 void launch_leaf_panel(const LeafFactorTask<T> *tasks, int count, int max_n, int nb, int k0,
                        int panel, int *info, cudaStream_t s) {
   if (count <= 0) return;
+  // register-resident panel: rows <= 512 RPT with 64 values per thread
+  const int rows = max_n - k0;
+  if constexpr (sizeof(T) == 4) {
+    if (nb == 64 && rows <= kRegThreads)
+      return launch_leaf_panel_reg<T, 64, 1>(tasks, count, k0, panel, info, s);
+    if (nb == 32 && rows <= 2 * kRegThreads)
+      return launch_leaf_panel_reg<T, 32, 2>(tasks, count, k0, panel, info, s);
+  } else {
+    if (nb == 32 && rows <= kRegThreads)
+      return launch_leaf_panel_reg<T, 32, 1>(tasks, count, k0, panel, info, s);
+    if (nb == 16 && rows <= 2 * kRegThreads)
+      return launch_leaf_panel_reg<T, 16, 2>(tasks, count, k0, panel, info, s);
+  }
   if (sizeof(T) == 8) {
     if (nb == 32) launch_leaf_panel_nb<T, 32>(tasks, count, max_n, k0, panel, info, s);
     else launch_leaf_panel_nb<T, 16>(tasks, count, max_n, k0, panel, info, s);
@@ -297,6 +745,35 @@ void launch_leaf_laswp(const LeafFactorTask<T> *tasks, int count, int max_cols, 
   HODLR_LAUNCH_CHECK();
 }
 
+template <typename T, int MC>
+void launch_leaf_apply_mc(const LeafFactorTask<T> *tasks, int count, int max_n, int max_cols,
+                          int nb, cudaStream_t s) {
+  constexpr int XS = MC + 16 / sizeof(T);
+  const size_t smem = ((size_t)max_n * XS + (size_t)nb * (nb + 1)) * sizeof(T);
+  HODLR_CUDA_TRY(cudaFuncSetAttribute(leaf_apply_kernel<T, MC>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(cdiv(max_cols, MC), count);
+  leaf_apply_kernel<T, MC><<<grid, kApplyThreads, smem, s>>>(tasks, nb, max_n);
+  HODLR_LAUNCH_CHECK();
+}
+
+template <typename T>
+void launch_leaf_apply(const LeafFactorTask<T> *tasks, int count, int max_n, int max_cols, int nb,
+                       cudaStream_t s) {
+  if (count <= 0 || max_cols <= 0 || max_n <= 0) return;
+  if (nb > 64) throw CudaError{cudaErrorInvalidValue};
+  // the chunk of P X is max_n x (MC + pad) in shared memory (<= 160 KB)
+  const bool wide_ok = ((size_t)max_n * (32 + 16 / sizeof(T)) + (size_t)nb * (nb + 1)) *
+                           sizeof(T) <= 180 * 1024;
+  if (max_cols <= 8) launch_leaf_apply_mc<T, 8>(tasks, count, max_n, max_cols, nb, s);
+  else if (max_cols <= 16 || !wide_ok) launch_leaf_apply_mc<T, 16>(tasks, count, max_n, max_cols, nb, s);
+  else launch_leaf_apply_mc<T, 32>(tasks, count, max_n, max_cols, nb, s);
+}
+
+template void launch_leaf_apply<double>(const LeafFactorTask<double> *, int, int, int, int,
+                                        cudaStream_t);
+template void launch_leaf_apply<float>(const LeafFactorTask<float> *, int, int, int, int,
+                                       cudaStream_t);
 template void launch_leaf_init<double>(const LeafFactorTask<double> *, int, int *, cudaStream_t);
 template void launch_leaf_init<float>(const LeafFactorTask<float> *, int, int *, cudaStream_t);
 template void launch_leaf_panel<double>(const LeafFactorTask<double> *, int, int, int, int, int,

@@ -30,6 +30,13 @@ struct LeafFactorTask {
   int pad;
 };
 
+// X <- (P L U)^{-1} X on every leaf with the blocked factors of a previous
+// factorization (LU in D, final row order in perm, per-panel Linv / Uinv);
+// X has task.ncols columns.  One CTA per (leaf, column chunk).
+template <typename T>
+void launch_leaf_apply(const LeafFactorTask<T> *tasks, int count, int max_n, int max_cols, int nb,
+                       cudaStream_t s);
+
 template <typename T>
 void launch_leaf_init(const LeafFactorTask<T> *tasks, int count, int *info, cudaStream_t s);
 template <typename T>

@@ -1,26 +1,30 @@
-// node.cu -- capacitance (node) solves, FP64, batched over a tree level.
+// node.cu -- capacitance (node) factorization, FP64, batched over a tree level.
 //
 // GPU restatement of LUSolveTask::cpu_task (src/solver/solver_tasks.cc:
 // 139-305) and of the 2r x 2r Schur system of serial_leaf_solve's internal
 // branch (solver_tasks.cc:483-535).  For a node with children b0, b1 and the
-// summed reduce results W0 = [V0Td0 | V0Tu0], W1 = [V1Td1 | V1Tu1]:
+// summed reduce results W0 = [V0Td0 | V0Tu0], W1 = [V1Td1 | V1Tu1] the
+// reference computes, per column block of the d part,
 //
-//   node_factor_kernel  one CTA per node.  Form 0: S = I - V1Tu1 V0Tu0 has
-//                       been written into S_lu by a batched GEMM launch; form
-//                       1 assembles [[V0Tu0, I], [I, V1Tu1]] here.  Factors S
-//                       with partial pivoting (LAPACK getrf semantics, lowest
-//                       index on ties), stores the LU and pivots, then forms
-//                       S^{-1} = U^{-1} L^{-1} P from the factors (in-place
-//                       triangular inverses in shared memory) and keeps both
-//                       V^T u blocks for later solves with the same factors.
-//   node_apply_kernel   grid (column chunk, node).  Form 0, as the
-//                       reference's dgemm / dgesv sequence:
-//                         T    = V1Td1 - V1Tu1 V0Td0   (dgemm at 236)
-//                         eta0 = S^{-1} T              (dgesv at 281)
-//                         eta1 = V0Td0 - V0Tu0 eta0    (dgemm at 299)
-//                       form 1: [eta0; eta1] = S^{-1} [V0Td0; V1Td1].
-//                       The three products run from shared memory, so the
-//                       kernel is fully parallel over columns and nodes.
+//   T    = V1Td1 - V1Tu1 V0Td0          (dgemm at 236)
+//   eta0 = S^{-1} T,  S = I - V1Tu1 V0Tu0   (dgemm at 261, dgesv at 281)
+//   eta1 = V0Td0 - V0Tu0 eta0           (dgemm at 299)
+//
+// which is linear in [V0Td0; V1Td1]:
+//
+//   [eta0; eta1] = M [V0Td0; V1Td1],
+//   M = [[ -S^{-1} V1Tu1,            S^{-1}         ],
+//        [ I + V0Tu0 S^{-1} V1Tu1,  -V0Tu0 S^{-1}   ]]
+//
+// (form 1, the 2r x 2r system [[V0Tu0, I], [I, V1Tu1]] of the leaf-internal
+// branch: M is that matrix's inverse).  node_factor_kernel forms M once per
+// node -- one CTA per node, S^{-1} by Gauss-Jordan elimination with partial
+// pivoting in shared memory (pivot = largest |a|, lowest row on ties, as
+// LAPACK's idamax), the three products from shared memory and L2 -- and the
+// solver applies M to every column block as one batched GEMM per level (the
+// same engine as the reduce and broadcast), for the fused pass and for every
+// later solve with the same factors.  INFO > 0 reports an exactly zero pivot
+// (singular S), as dgesv.
 #include "common.cuh"
 #include "node.cuh"
 
@@ -28,56 +32,108 @@ namespace hodlr {
 
 namespace {
 
-constexpr int kNodeThreads = 256;
-constexpr int kApplyCols = 32;
+constexpr int kNodeThreads = 1024;
+constexpr int kNodeWarps = kNodeThreads / 32;
+
+}  // namespace
+
+// doubles of the factor kernel's shared memory before the staged operands:
+// A (s x (s + 1)), rowk, colk (s each), piv, src (s ints each), rounded up
+__host__ __device__ size_t node_factor_words(int max_s) {
+  return (size_t)max_s * (max_s + 1) + 2 * (size_t)max_s + (size_t)max_s + 2;
+}
+
+namespace {
+
+// out(i, c) = [i == c] (if add_identity) + alpha * sum_k a(i, k) b(k, c) for
+// i < rows, c < cols: lanes over rows, warps over columns, 2 x 2 outputs per
+// thread and pass.
+template <typename FA, typename FB, typename FO>
+__device__ inline void node_product(int rows, int cols, int K, double alpha, bool add_identity,
+                                    FA a, FB b, FO out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i0 = lane; i0 < rows; i0 += 64) {
+    const int i1 = i0 + 32 < rows ? i0 + 32 : i0;
+    for (int c0 = warp; c0 < cols; c0 += 2 * kNodeWarps) {
+      const int c1 = c0 + kNodeWarps < cols ? c0 + kNodeWarps : c0;
+      double a00 = 0.0, a01 = 0.0, a10 = 0.0, a11 = 0.0;
+#pragma unroll 8
+      for (int k = 0; k < K; ++k) {
+        const double x0 = a(i0, k), x1 = a(i1, k);
+        const double y0 = b(k, c0), y1 = b(k, c1);
+        a00 += x0 * y0;
+        a01 += x0 * y1;
+        a10 += x1 * y0;
+        a11 += x1 * y1;
+      }
+      auto put = [&](int i, int c, double v) {
+        out(i, c, (add_identity && i == c ? 1.0 : 0.0) + alpha * v);
+      };
+      put(i0, c0, a00);
+      if (c1 != c0) put(i0, c1, a01);
+      if (i1 != i0) {
+        put(i1, c0, a10);
+        if (c1 != c0) put(i1, c1, a11);
+      }
+    }
+  }
+}
 
 template <typename TW, typename TE>
 __global__ void __launch_bounds__(kNodeThreads)
-    node_factor_kernel(const NodeTask<TW, TE> *tasks, int form, int *info) {
+    node_factor_kernel(const NodeTask<TW, TE> *tasks, int form, int max_s, int max_r, int stage,
+                       int *info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const NodeTask<TW, TE> tk = tasks[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int r0 = tk.r0, r1 = tk.r1;
-  const int s = form == 0 ? r0 : r0 + r1;
-  double *S = reinterpret_cast<double *>(smem_raw);  // s x s, column-major
-  int *piv = reinterpret_cast<int *>(S + (size_t)s * s);
-  int *perm = piv + s;
+  const int r0 = tk.r0, r1 = tk.r1, s2 = r0 + r1;
+  const int s = form == 0 ? r0 : s2;
+  const int lda = s + 1;                              // row stride (odd: no bank conflicts)
+  double *A = reinterpret_cast<double *>(smem_raw);   // s x s, row-major
+  double *rowk = A + (size_t)s * lda;
+  double *colk = rowk + s;
+  int *piv = reinterpret_cast<int *>(colk + s);
+  int *src = piv + s;
+  // form 0 with stage != 0: V0Tu0, V1Tu1 and G0 as FP64 in shared memory
+  double *W0s = reinterpret_cast<double *>(smem_raw) + node_factor_words(max_s);
+  double *W1s = W0s + (size_t)max_r * max_r;
+  double *Gs = W1s + (size_t)max_r * max_r;
   __shared__ int s_info;
 
-  // keep V0^T u0 (r1 x r0) and V1^T u1 (r0 x r1) for solves with these factors
-  for (int e = tid; e < r1 * r0; e += kNodeThreads) {
-    const int i = e % r1, j = e / r1;
-    tk.VTu0[e] = double(tk.W0u[i + (long long)j * tk.ldw0u]);
-  }
-  for (int e = tid; e < r0 * r1; e += kNodeThreads) {
-    const int i = e % r0, j = e / r0;
-    tk.VTu1[e] = double(tk.W1u[i + (long long)j * tk.ldw1u]);
-  }
   if (tid == 0) s_info = 0;
-  if (form == 0) {
-    for (int e = tid; e < s * s; e += kNodeThreads) S[e] = tk.S_lu[e];
-  } else {
-    for (int e = tid; e < s * s; e += kNodeThreads) S[e] = 0.0;
-    __syncthreads();
-    for (int i = tid; i < s; i += kNodeThreads) S[(r1 + i) % s + (size_t)i * s] = 1.0;
+  if (form == 0 && stage) {
     for (int e = tid; e < r1 * r0; e += kNodeThreads) {
       const int i = e % r1, j = e / r1;
-      S[i + (size_t)j * s] = double(tk.W0u[i + (long long)j * tk.ldw0u]);
+      W0s[e] = double(tk.W0u[i + (long long)j * tk.ldw0u]);
     }
     for (int e = tid; e < r0 * r1; e += kNodeThreads) {
       const int i = e % r0, j = e / r0;
-      S[(r1 + i) + (size_t)(r0 + j) * s] = double(tk.W1u[i + (long long)j * tk.ldw1u]);
+      W1s[e] = double(tk.W1u[i + (long long)j * tk.ldw1u]);
+    }
+  }
+  if (form == 0) {
+    for (int e = tid; e < s * s; e += kNodeThreads) {
+      const int i = e % s, c = e / s;
+      A[i * lda + c] = tk.S[e];
+    }
+  } else {
+    for (int e = tid; e < s * s; e += kNodeThreads) {
+      const int i = e % s, c = e / s;
+      double v = (i == (r1 + c) % s) ? 1.0 : 0.0;
+      if (i < r1 && c < r0) v = double(tk.W0u[i + (long long)c * tk.ldw0u]);
+      else if (i >= r1 && c >= r0) v = double(tk.W1u[(i - r1) + (long long)(c - r0) * tk.ldw1u]);
+      A[i * lda + c] = v;
     }
   }
   __syncthreads();
 
-  // ---- LU with partial pivoting; warp 0 picks and swaps the pivot row
-  for (int j = 0; j < s; ++j) {
+  // ---- Gauss-Jordan: A <- (P S)^{-1} in place, two barriers per column
+  for (int k = 0; k < s; ++k) {
     if (warp == 0) {
       double best = -1.0;
       int bi = s;
-      for (int i = j + lane; i < s; i += 32) {
-        const double a = fabs(S[i + (size_t)j * s]);
+      for (int i = k + lane; i < s; i += 32) {
+        const double a = fabs(A[i * lda + k]);
         if (a > best) { best = a; bi = i; }
       }
 #pragma unroll
@@ -87,203 +143,134 @@ __global__ void __launch_bounds__(kNodeThreads)
         if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
       }
       bi = __shfl_sync(0xffffffffu, bi, 0);
-      if (bi >= s) bi = j;
-      if (bi != j)
+      if (bi >= s) bi = k;  // NaN column: keep the diagonal
+      if (bi != k)
         for (int c = lane; c < s; c += 32) {
-          const double t = S[j + (size_t)c * s];
-          S[j + (size_t)c * s] = S[bi + (size_t)c * s];
-          S[bi + (size_t)c * s] = t;
+          const double t = A[k * lda + c];
+          A[k * lda + c] = A[bi * lda + c];
+          A[bi * lda + c] = t;
         }
+      __syncwarp();
+      for (int c = lane; c < s; c += 32) rowk[c] = A[k * lda + c];
+      for (int i = lane; i < s; i += 32) colk[i] = A[i * lda + k];
       if (lane == 0) {
-        piv[j] = bi;
-        if (S[j + (size_t)j * s] == 0.0 && s_info == 0) s_info = j + 1;
+        piv[k] = bi;
+        if (A[k * lda + k] == 0.0 && s_info == 0) s_info = k + 1;
       }
     }
     __syncthreads();
-    const double pv = S[j + (size_t)j * s];
-    if (pv != 0.0) {
-      const double rinv = 1.0 / pv;
-      for (int row = j + 1 + tid; row < s; row += kNodeThreads) {
-        const double l = S[row + (size_t)j * s] * rinv;
-        for (int c = j + 1; c < s; ++c) S[row + (size_t)c * s] -= l * S[j + (size_t)c * s];
-        S[row + (size_t)j * s] = l;
+    const double pk = rowk[k];
+    if (pk != 0.0) {
+      const double rinv = 1.0 / pk;
+      for (int i = warp; i < s; i += kNodeWarps) {
+        const double f = colk[i] * rinv;
+        double *Ai = A + i * lda;
+        if (i == k) {
+          for (int c = lane; c < s; c += 32) Ai[c] = (c == k ? 1.0 : rowk[c]) * rinv;
+        } else {
+          for (int c = lane; c < s; c += 32)
+            Ai[c] = (c == k ? 0.0 : Ai[c]) - f * (c == k ? 1.0 : rowk[c]);
+        }
       }
     }
     __syncthreads();
   }
-  for (int e = tid; e < s * s; e += kNodeThreads) tk.S_lu[e] = S[e];
-  for (int i = tid; i < s; i += kNodeThreads) tk.S_piv[i] = piv[i];
   if (tid == 0) {
     if (info) info[tk.info_slot] = s_info;
-    for (int i = 0; i < s; ++i) perm[i] = i;
-    for (int j = 0; j < s; ++j) {
-      const int p = piv[j];
-      if (p != j) { const int t = perm[j]; perm[j] = perm[p]; perm[p] = t; }
+    // undo the row interchanges as column interchanges, last pivot first
+    for (int j = 0; j < s; ++j) src[j] = j;
+    for (int k = s - 1; k >= 0; --k) {
+      const int p = piv[k];
+      const int t = src[k];
+      src[k] = src[p];
+      src[p] = t;
     }
   }
   __syncthreads();
-  if (s_info != 0) return;  // singular: no inverse (uniform across the CTA)
-
-  // ---- L^{-1} in place (unit lower), columns right to left
-  for (int j = s - 2; j >= 0; --j) {
-    double v = 0.0;
-    const int i = j + 1 + tid;
-    if (i < s) {
-      v = S[i + (size_t)j * s];
-      for (int k = j + 1; k < i; ++k) v += S[i + (size_t)k * s] * S[k + (size_t)j * s];
-      v = -v;
+  if (s_info != 0) return;  // singular: no solve matrix (uniform across the CTA)
+  // S^{-1}(i, j) = A[i][src[j]]
+  const long long ldm = s2;
+  TE *M = tk.M;
+  if (form == 1) {
+    for (int e = tid; e < s * s; e += kNodeThreads) {
+      const int i = e % s, j = e / s;
+      M[i + (long long)j * ldm] = TE(A[i * lda + src[j]]);
     }
-    __syncthreads();
-    if (i < s) S[i + (size_t)j * s] = v;
-    __syncthreads();
+    return;
   }
-  // ---- U^{-1} in place (upper), columns left to right
-  for (int j = 0; j < s; ++j) {
-    const double ujj = S[j + (size_t)j * s];
-    double v = 0.0;
-    const int i = tid;
-    if (i < j) {
-      for (int k = i; k < j; ++k) v += S[i + (size_t)k * s] * S[k + (size_t)j * s];
-      v = -v / ujj;
-    }
-    __syncthreads();
-    if (i < j) S[i + (size_t)j * s] = v;
-    if (i == j) S[j + (size_t)j * s] = 1.0 / ujj;
-    __syncthreads();
-  }
-  // ---- S^{-1}[:, perm[q]] = (U^{-1} L^{-1})[:, q]
-  for (int e = tid; e < s * s; e += kNodeThreads) {
-    const int i = e % s, q = e / s;
-    double acc = 0.0;
-    for (int k = max(i, q); k < s; ++k) {
-      const double lk = (k == q) ? 1.0 : S[k + (size_t)q * s];
-      acc += S[i + (size_t)k * s] * lk;
-    }
-    tk.S_inv[i + (size_t)perm[q] * s] = acc;
-  }
-}
-
-// Y (M x cc, ld ldy) = Y0 (or 0) + alpha * A (M x K, ld M) * X (K x cc, ld
-// ldx); all in shared memory, Y aliases neither A nor X.
-__device__ inline void smem_gemm(double *Y, int ldy, const double *Y0, int ldy0, double alpha,
-                                 const double *A, int M, int K, const double *X, int ldx, int cc) {
-  for (int e = threadIdx.x; e < M * cc; e += kNodeThreads) {
-    const int i = e % M, c = e / M;
-    double acc = 0.0;
-    const double *xc = X + (size_t)c * ldx;
-#pragma unroll 4
-    for (int k = 0; k < K; ++k) acc += A[i + (size_t)k * M] * xc[k];
-    Y[i + (size_t)c * ldy] = (Y0 ? Y0[i + (size_t)c * ldy0] : 0.0) + alpha * acc;
-  }
-}
-
-template <typename TE>
-__device__ inline void store_eta(TE *eta, long long ld, int cb, const double *Y, int ldy, int M,
-                                 int cc) {
-  for (int e = threadIdx.x; e < M * cc; e += kNodeThreads) {
-    const int i = e % M, c = e / M;
-    eta[i + (long long)(cb + c) * ld] = TE(Y[i + (size_t)c * ldy]);
-  }
-}
-
-template <typename TW, typename TE>
-__global__ void __launch_bounds__(kNodeThreads)
-    node_apply_kernel(const NodeTask<TW, TE> *tasks, int form) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const NodeTask<TW, TE> tk = tasks[blockIdx.y];
-  const int cb = blockIdx.x * kApplyCols;
-  if (cb >= tk.c) return;
-  const int cc = min(kApplyCols, tk.c - cb);
-  const int tid = threadIdx.x;
-  const int r0 = tk.r0, r1 = tk.r1;
-  const int s = form == 0 ? r0 : r0 + r1;
-  const int rs = r0 + r1;
-  double *A = reinterpret_cast<double *>(smem_raw);  // staged matrix, <= s x s
-  double *R = A + (size_t)s * s;                     // rs x kApplyCols: [V0Td0; V1Td1]
-  double *T = R + (size_t)rs * kApplyCols;           // form 0: max(r0, r1) x kApplyCols
-  for (int e = tid; e < r1 * cc; e += kNodeThreads) {
-    const int i = e % r1, j = e / r1;
-    R[i + (size_t)j * rs] = double(tk.W0d[i + (long long)(cb + j) * tk.ldw0d]);
-  }
-  for (int e = tid; e < r0 * cc; e += kNodeThreads) {
+  // form 0: the blocks of M around S^{-1} (r0 x r0)
+  for (int e = tid; e < r0 * r0; e += kNodeThreads) {
     const int i = e % r0, j = e / r0;
-    R[r1 + i + (size_t)j * rs] = double(tk.W1d[i + (long long)(cb + j) * tk.ldw1d]);
+    M[i + (long long)(r1 + j) * ldm] = TE(A[i * lda + src[j]]);
   }
-  if (form == 0) {
-    for (int e = tid; e < r0 * r1; e += kNodeThreads) A[e] = tk.VTu1[e];
+  if (stage) {
+    // G0 = -S^{-1} V1Tu1 (r0 x r1): M's upper left block, kept for the last product
+    node_product(
+        r0, r1, r0, -1.0, false, [&](int i, int k) { return A[i * lda + src[k]]; },
+        [&](int k, int c) { return W1s[k + c * r0]; },
+        [&](int i, int c, double v) {
+          Gs[i + c * r0] = v;
+          M[i + (long long)c * ldm] = TE(v);
+        });
+    // -V0Tu0 S^{-1} (r1 x r0): M's lower right block
+    node_product(
+        r1, r0, r0, -1.0, false, [&](int i, int k) { return W0s[i + k * r1]; },
+        [&](int k, int c) { return A[k * lda + src[c]]; },
+        [&](int i, int c, double v) { M[(r0 + i) + (long long)(r1 + c) * ldm] = TE(v); });
     __syncthreads();
-    // T = V1Td1 - V1Tu1 V0Td0
-    smem_gemm(T, r0, R + r1, rs, -1.0, A, r0, r1, R, rs, cc);
-    __syncthreads();
-    for (int e = tid; e < r0 * r0; e += kNodeThreads) A[e] = tk.S_inv[e];
-    __syncthreads();
-    // eta0 = S^{-1} T into the V1Td1 rows of R
-    smem_gemm(R + r1, rs, nullptr, 0, 1.0, A, r0, r0, T, r0, cc);
-    __syncthreads();
-    for (int e = tid; e < r1 * r0; e += kNodeThreads) A[e] = tk.VTu0[e];
-    __syncthreads();
-    // eta1 = V0Td0 - V0Tu0 eta0 into T
-    smem_gemm(T, r1, R, rs, -1.0, A, r1, r0, R + r1, rs, cc);
-    __syncthreads();
-    store_eta(tk.eta0, tk.ld_eta0, cb, R + r1, rs, r0, cc);
-    store_eta(tk.eta1, tk.ld_eta1, cb, T, r1, r1, cc);
-  } else {
-    for (int e = tid; e < s * s; e += kNodeThreads) A[e] = tk.S_inv[e];
-    __syncthreads();
-    // [eta0; eta1] = S^{-1} [V0Td0; V1Td1], straight to global
-    for (int e = tid; e < s * cc; e += kNodeThreads) {
-      const int i = e % s, c = e / s;
-      double acc = 0.0;
-      const double *xc = R + (size_t)c * rs;
-#pragma unroll 4
-      for (int k = 0; k < s; ++k) acc += A[i + (size_t)k * s] * xc[k];
-      if (i < r0) tk.eta0[i + (long long)(cb + c) * tk.ld_eta0] = TE(acc);
-      else tk.eta1[(i - r0) + (long long)(cb + c) * tk.ld_eta1] = TE(acc);
-    }
+    // I - V0Tu0 G0 (r1 x r1): M's lower left block
+    node_product(
+        r1, r1, r0, -1.0, true, [&](int i, int k) { return W0s[i + k * r1]; },
+        [&](int k, int c) { return Gs[k + c * r0]; },
+        [&](int i, int c, double v) { M[(r0 + i) + (long long)c * ldm] = TE(v); });
+    return;
   }
+  const TW *W0u = tk.W0u, *W1u = tk.W1u;
+  const long long l0 = tk.ldw0u, l1 = tk.ldw1u;
+  double *F = tk.F;
+  // F = -V0Tu0 S^{-1} (r1 x r0): M's lower right block and FP64 work copy
+  node_product(
+      r1, r0, r0, -1.0, false, [&](int i, int k) { return double(W0u[i + k * l0]); },
+      [&](int k, int c) { return A[k * lda + src[c]]; },
+      [&](int i, int c, double v) {
+        F[i + (long long)c * r1] = v;
+        M[(r0 + i) + (long long)(r1 + c) * ldm] = TE(v);
+      });
+  // G0 = -S^{-1} V1Tu1 (r0 x r1): M's upper left block
+  node_product(
+      r0, r1, r0, -1.0, false, [&](int i, int k) { return A[i * lda + src[k]]; },
+      [&](int k, int c) { return double(W1u[k + c * l1]); },
+      [&](int i, int c, double v) { M[i + (long long)c * ldm] = TE(v); });
+  __syncthreads();  // F (global) visible to the whole CTA
+  // I - V0Tu0 G0 = I + V0Tu0 S^{-1} V1Tu1 = I - F V1Tu1 (r1 x r1): M's lower left block
+  node_product(
+      r1, r1, r0, -1.0, true, [&](int i, int k) { return F[i + (long long)k * r1]; },
+      [&](int k, int c) { return double(W1u[k + c * l1]); },
+      [&](int i, int c, double v) { M[(r0 + i) + (long long)c * ldm] = TE(v); });
 }
 
 }  // namespace
 
-size_t node_factor_smem(int max_s) {
-  return (size_t)max_s * max_s * sizeof(double) + 2 * (size_t)max_s * sizeof(int) + 16;
-}
-size_t node_apply_smem(int max_s, int max_rs, int form) {
-  // A (s x s) + R (rs x 32) + T (form 0 only, <= rs x 32)
-  return (size_t)max_s * max_s * sizeof(double) + (size_t)max_rs * kApplyCols * sizeof(double) +
-         (form == 0 ? (size_t)max_rs * kApplyCols * sizeof(double) : 0) + 16;
-}
+size_t node_factor_smem(int max_s) { return node_factor_words(max_s) * sizeof(double); }
 
 template <typename TW, typename TE>
-void launch_node_factor(const NodeTask<TW, TE> *tasks, int count, int max_s, int form,
+void launch_node_factor(const NodeTask<TW, TE> *tasks, int count, int max_s, int max_r, int form,
                         int *info, cudaStream_t s) {
   if (count <= 0) return;
-  const size_t smem = node_factor_smem(max_s);
+  size_t smem = node_factor_smem(max_s);
+  const size_t staged = smem + 3 * (size_t)max_r * max_r * sizeof(double);
+  const int stage = (form == 0 && staged <= 200 * 1024) ? 1 : 0;
+  if (stage) smem = staged;
   HODLR_CUDA_TRY(cudaFuncSetAttribute(node_factor_kernel<TW, TE>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  node_factor_kernel<TW, TE><<<count, kNodeThreads, smem, s>>>(tasks, form, info);
-  HODLR_LAUNCH_CHECK();
-}
-
-template <typename TW, typename TE>
-void launch_node_apply(const NodeTask<TW, TE> *tasks, int count, int max_s, int max_rs,
-                       int max_c, int form, cudaStream_t s) {
-  if (count <= 0 || max_c <= 0) return;
-  const size_t smem = node_apply_smem(max_s, max_rs, form);
-  HODLR_CUDA_TRY(cudaFuncSetAttribute(node_apply_kernel<TW, TE>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid(cdiv(max_c, kApplyCols), count);
-  node_apply_kernel<TW, TE><<<grid, kNodeThreads, smem, s>>>(tasks, form);
+  node_factor_kernel<TW, TE><<<count, kNodeThreads, smem, s>>>(tasks, form, max_s, max_r, stage,
+                                                                info);
   HODLR_LAUNCH_CHECK();
 }
 
 template void launch_node_factor<double, double>(const NodeTask<double, double> *, int, int,
-                                                 int, int *, cudaStream_t);
+                                                 int, int, int *, cudaStream_t);
 template void launch_node_factor<float, float>(const NodeTask<float, float> *, int, int, int,
-                                               int *, cudaStream_t);
-template void launch_node_apply<double, double>(const NodeTask<double, double> *, int, int, int,
-                                                int, int, cudaStream_t);
-template void launch_node_apply<float, float>(const NodeTask<float, float> *, int, int, int, int,
-                                              int, cudaStream_t);
+                                               int, int *, cudaStream_t);
 
 }  // namespace hodlr

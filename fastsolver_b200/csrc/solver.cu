@@ -43,7 +43,9 @@ struct PathSpec {
   T *part = nullptr;   // split-K partial slots
   T *wfin = nullptr;   // summed W per child (when a child has several slots)
   TE *eta = nullptr;
+  TE *M = nullptr;     // per-node solve matrices, (2r)^2 each
   NodeStore *ns = nullptr;
+  const LeafPlan<T> *factors = nullptr;  // apply paths: the blocked leaf factors
   bool factor = false;
   int red_chunk = 512, bc_chunk = 512;
 };
@@ -115,6 +117,7 @@ void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long
     lp.laswp_cols = std::max(lp.laswp_cols, k.n + k.ncols);
   }
   lp.tasks.upload(tasks);
+  lp.host_tasks = tasks;
   lp.nleaf = nleaf;
   lp.fwd.clear();
   lp.bwd.clear();
@@ -221,8 +224,21 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
   }
   plan.nleaf = (int)lt.size();
   plan.leaf_tasks.upload(lt);
-  if (sp.factor)
+  if (sp.factor) {
     build_leaf_plan<T>(t, sp.D, sp.ldd, sp.X, sp.ldx, sp.ipiv, sp.perm, true, m, plan.leaf);
+  } else if (sp.factors) {
+    std::vector<LeafFactorTask<T>> at = sp.factors->host_tasks;
+    for (size_t q = 0; q < at.size(); ++q) {
+      const Node &n = t.nodes[t.leaves[q]];
+      at[q].X = sp.X + n.row_beg;
+      at[q].ldx = sp.ldx;
+      at[q].ncols = m;
+    }
+    plan.apply_tasks.upload(at);
+    plan.apply_nb = sp.factors->nb;
+    plan.apply_max_n = sp.factors->max_n;
+    plan.apply_max_cols = m;
+  }
   const int nleaf = (int)t.leaves.size();
 
   for (int d = t.max_depth - 1; d >= 0; --d) {
@@ -235,12 +251,16 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
     std::vector<SumTask<T>> su;
     std::vector<GemmItem<T, double>> gi;
     std::vector<GemmSeg<T>> gs;
+    std::vector<GemmItem<T, T>> ai;
+    std::vector<GemmSeg<T>> as;
     size_t poff = 0, woff = 0, eoff = 0;
     for (int p : ids) {
       const Node &P = t.nodes[p];
       const Node &c0 = t.nodes[P.lchild], &c1 = t.nodes[P.rchild];
       const int cw = sp.factor ? c0.col_beg : m;
       NodeTask<T, TE> k{};
+      const T *W0d = nullptr, *W1d = nullptr;
+      long long ldw0d = 0, ldw1d = 0;
       for (int side = 0; side < 2; ++side) {
         const Node &c = side ? c1 : c0;
         const int NW = sp.factor ? c.col_beg + c.ncol : m;
@@ -285,65 +305,85 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
           L->sum_max_len = std::max(L->sum_max_len, st.len);
         }
         if (side == 0) {
-          k.W0d = W; k.W0u = W + (size_t)M * (NW - c.ncol);
-          k.ldw0d = k.ldw0u = M; k.np0 = 1;
+          W0d = W; k.W0u = W + (size_t)M * (NW - c.ncol);
+          ldw0d = k.ldw0u = M;
         } else {
-          k.W1d = W; k.W1u = W + (size_t)M * (NW - c.ncol);
-          k.ldw1d = k.ldw1u = M; k.np1 = 1;
+          W1d = W; k.W1u = W + (size_t)M * (NW - c.ncol);
+          ldw1d = k.ldw1u = M;
         }
       }
-      k.r0 = c0.ncol;
-      k.r1 = c1.ncol;
-      k.c = cw;
-      k.eta0 = sp.eta + eoff;
-      k.ld_eta0 = k.r0;
-      eoff += (size_t)k.r0 * cw;
-      k.eta1 = sp.eta + eoff;
-      k.ld_eta1 = k.r1;
-      eoff += (size_t)k.r1 * cw;
-      k.S_lu = sp.ns->S_lu.p + (size_t)p * sp.ns->s_slot;
-      k.S_inv = sp.ns->S_inv.p + (size_t)p * sp.ns->s_slot;
-      k.S_piv = sp.ns->S_piv.p + (size_t)p * sp.ns->s_max;
-      k.VTu0 = sp.ns->VTu0.p + (size_t)p * sp.ns->rr;
-      k.VTu1 = sp.ns->VTu1.p + (size_t)p * sp.ns->rr;
+      const int r0 = c0.ncol, r1 = c1.ncol, s2 = r0 + r1;
+      k.r0 = r0;
+      k.r1 = r1;
+      // eta = [eta0; eta1] (s2 x cw, ld s2): eta0 feeds child 0, eta1 child 1
+      TE *eta = sp.eta + eoff;
+      eoff += (size_t)s2 * cw;
+      k.S = sp.ns->S.p + (size_t)p * sp.ns->rr;
+      k.F = sp.ns->F.p + (size_t)p * sp.ns->rr;
+      k.M = sp.M + (size_t)p * sp.ns->mm;
       k.info_slot = nleaf + p;
       nt.push_back(k);
       if (sp.factor && form == 0) {
-        // S = I - V1Tu1 V0Tu0 (r0 x r0, ld r0) into the node's S_lu slot
+        // S = I - V1Tu1 V0Tu0 (r0 x r0, ld r0): the dgemm at solver_tasks.cc:261
         GemmSeg<T> g{};
         g.A = k.W1u;
         g.lda = k.ldw1u;
         g.B = k.W0u;
         g.ldb = k.ldw0u;
-        g.K = k.r1;
+        g.K = r1;
         GemmItem<T, double> it{};
-        it.C = k.S_lu;
-        it.ldc = k.r0;
+        it.C = sp.ns->S.p + (size_t)p * sp.ns->rr;
+        it.ldc = r0;
         it.Cin = sp.ns->ident.p;
-        it.ldcin = sp.ns->s_max;
-        it.M = it.N = k.r0;
+        it.ldcin = t.rank;
+        it.M = it.N = r0;
         it.seg_begin = (int)gs.size();
         it.seg_count = 1;
         gs.push_back(g);
         gi.push_back(it);
-        L->gram_max = std::max(L->gram_max, k.r0);
+        L->gram_max = std::max(L->gram_max, r0);
       }
-      const int s = form == 0 ? k.r0 : k.r0 + k.r1;
+      const int s = form == 0 ? r0 : s2;
       L->max_s = std::max(L->max_s, s);
-      L->max_rs = std::max(L->max_rs, k.r0 + k.r1);
-      L->max_c = std::max(L->max_c, cw);
+      L->max_r = std::max(L->max_r, std::max(r0, r1));
+      if (cw > 0) {
+        // [eta0; eta1] = M [V0Td0; V1Td1]: one item, two K segments
+        GemmSeg<T> a0{}, a1{};
+        a0.A = reinterpret_cast<const T *>(k.M);
+        a0.lda = s2;
+        a0.B = W0d;
+        a0.ldb = ldw0d;
+        a0.K = r1;
+        a1.A = reinterpret_cast<const T *>(k.M) + (size_t)r1 * s2;
+        a1.lda = s2;
+        a1.B = W1d;
+        a1.ldb = ldw1d;
+        a1.K = r0;
+        GemmItem<T, T> it{};
+        it.C = reinterpret_cast<T *>(eta);
+        it.ldc = s2;
+        it.M = s2;
+        it.N = cw;
+        it.seg_begin = (int)as.size();
+        it.seg_count = 2;
+        as.push_back(a0);
+        as.push_back(a1);
+        ai.push_back(it);
+        L->ap_max_m = std::max(L->ap_max_m, s2);
+        L->ap_max_n = std::max(L->ap_max_n, cw);
+      }
       // broadcast d_c -= u_c eta into both children
       for (int side = 0; side < 2; ++side) {
         const Node &c = side ? c1 : c0;
-        const TE *eta = side ? k.eta1 : k.eta0;
+        const TE *eta_c = side ? eta + r0 : eta;
         if (cw == 0) continue;
         for (int rb = c.row_beg; rb < c.row_beg + c.nrow; rb += sp.bc_chunk) {
           const int rows = std::min(sp.bc_chunk, c.row_beg + c.nrow - rb);
           GemmSeg<T> sg{};
           sg.A = sp.Usrc + rb + (long long)c.col_beg * sp.ldu;
-          sg.B = reinterpret_cast<const T *>(eta);
+          sg.B = reinterpret_cast<const T *>(eta_c);
           sg.lda = sp.ldu;
-          sg.ldb = c.ncol;
+          sg.ldb = s2;
           sg.K = c.ncol;
           GemmItem<T, T> it{};
           it.C = sp.X + rb;
@@ -370,6 +410,9 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
     L->n_gram = (int)gi.size();
     L->node_tasks.upload(nt);
     L->n_nodes = (int)nt.size();
+    L->ap_items.upload(ai);
+    L->ap_segs.upload(as);
+    L->n_ap = (int)ai.size();
     L->bc_items.upload(bi);
     L->bc_segs.upload(bs);
     L->n_bc = (int)bi.size();
@@ -418,6 +461,10 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
   LeafTask<T> none{};
   if (plan.factor) {
     run_leaf_plan<T>(pf, plan.leaf, info, s);
+  } else if (plan.apply_nb > 0) {
+    PhaseScope ps(pf, PH_GETRS, s);
+    launch_leaf_apply<T>(plan.apply_tasks.p, plan.nleaf, plan.apply_max_n, plan.apply_max_cols,
+                         plan.apply_nb, s);
   } else {
     PhaseScope ps(pf, PH_GETRS, s);
     launch_getrs<T>(plan.leaf_tasks.p, none, plan.nleaf, plan.max_n, plan.max_nrhs, s);
@@ -435,11 +482,12 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
       if (form == 0)
         launch_gemm_items<T, double, double>(L.gram_items.p, L.gram_segs.p, L.n_gram, L.gram_max,
                                              L.gram_max, false, -1.0, 1.0, s);
-      launch_node_factor<T, TE>(L.node_tasks.p, L.n_nodes, L.max_s, form, info, s);
+      launch_node_factor<T, TE>(L.node_tasks.p, L.n_nodes, L.max_s, L.max_r, form, info, s);
     }
     {
       PhaseScope ps(pf, PH_NODE_APPLY, s);
-      launch_node_apply<T, TE>(L.node_tasks.p, L.n_nodes, L.max_s, L.max_rs, L.max_c, form, s);
+      launch_gemm_items<T, T, T>(L.ap_items.p, L.ap_segs.p, L.n_ap, L.ap_max_m, L.ap_max_n,
+                                 false, T(1), T(0), s);
     }
     {
       PhaseScope ps(pf, PH_BCAST, s);
@@ -449,20 +497,18 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
   }
 }
 
-void alloc_node_store(NodeStore &ns, const Tree &t) {
+void alloc_node_store(NodeStore &ns, const Tree &t, bool fp64) {
   const int r = t.rank;
-  ns.s_max = (2 * r <= kMaxNodeS) ? 2 * r : r;
-  ns.s_slot = ns.s_max * ns.s_max;
   ns.rr = r * r;
+  ns.mm = 4 * r * r;
   const size_t nn = t.nodes.size();
-  ns.S_lu.ensure(nn * ns.s_slot);
-  ns.S_inv.ensure(nn * ns.s_slot);
-  ns.S_piv.ensure(nn * ns.s_max);
-  std::vector<double> I((size_t)ns.s_max * ns.s_max, 0.0);
-  for (int i = 0; i < ns.s_max; ++i) I[(size_t)i * ns.s_max + i] = 1.0;
+  ns.S.ensure(nn * ns.rr);
+  ns.F.ensure(nn * ns.rr);
+  if (fp64) ns.M64.ensure(nn * ns.mm);
+  else ns.M32.ensure(nn * ns.mm);
+  std::vector<double> I((size_t)r * r, 0.0);
+  for (int i = 0; i < r; ++i) I[(size_t)i * r + i] = 1.0;
   ns.ident.upload(I);
-  ns.VTu0.ensure(nn * ns.rr);
-  ns.VTu1.ensure(nn * ns.rr);
 }
 
 void build_matvec(System &S, const double *x, MatvecPlan &mv) {
@@ -641,7 +687,7 @@ void System::ensure_fp64() {
   Y64.ensure(n * m);
   ipiv64.ensure(n);
   perm64.ensure(n);
-  alloc_node_store(ns64, tree);
+  alloc_node_store(ns64, tree, true);
   size_t pf, wf, ef, pa, wa, ea;
   path_need(tree, true, red_chunk, pf, wf, ef);
   path_need(tree, false, red_chunk, pa, wa, ea);
@@ -649,15 +695,15 @@ void System::ensure_fp64() {
   wfin64.ensure(std::max<size_t>(std::max(wf, wa), 1));
   eta64.ensure(std::max<size_t>(std::max(ef, ea), 1));
   for (int form = 0; form < 2; ++form) {
-    if (form == 1 && ns64.s_max < 2 * r) continue;
+    if (form == 1 && 2 * r > kMaxNodeS) continue;
     PathSpec<double, double> f;
     f.X = X64.p; f.ldx = N; f.Usrc = X64.p; f.ldu = N;
     f.D = DLU64.p; f.ldd = N; f.ipiv = ipiv64.p; f.perm = perm64.p;
-    f.V = V.p; f.ldv = N; f.part = part64.p; f.wfin = wfin64.p; f.eta = eta64.p; f.ns = &ns64;
+    f.V = V.p; f.ldv = N; f.part = part64.p; f.wfin = wfin64.p; f.eta = eta64.p; f.M = ns64.M64.p; f.ns = &ns64;
     f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk;
     build_path(tree, f, fused64[form], form);
     PathSpec<double, double> a = f;
-    a.X = Y64.p; a.factor = false;
+    a.X = Y64.p; a.factor = false; a.factors = &fused64[form].leaf;
     build_path(tree, a, apply64[form], form);
   }
 }
@@ -671,7 +717,7 @@ void System::ensure_mixed() {
   Y32.ensure(n * m);
   ipiv32.ensure(n);
   perm32.ensure(n);
-  alloc_node_store(ns32, tree);
+  alloc_node_store(ns32, tree, false);
   size_t pf, wf, ef, pa, wa, ea;
   path_need(tree, true, red_chunk, pf, wf, ef);
   path_need(tree, false, red_chunk, pa, wa, ea);
@@ -681,11 +727,11 @@ void System::ensure_mixed() {
   PathSpec<float, float> f;
   f.X = X32.p; f.ldx = N; f.Usrc = X32.p; f.ldu = N;
   f.D = D32.p; f.ldd = N; f.ipiv = ipiv32.p; f.perm = perm32.p;
-  f.V = V32.p; f.ldv = N; f.part = part32.p; f.wfin = wfin32.p; f.eta = eta32.p; f.ns = &ns32;
+  f.V = V32.p; f.ldv = N; f.part = part32.p; f.wfin = wfin32.p; f.eta = eta32.p; f.M = ns32.M32.p; f.ns = &ns32;
   f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk;
   build_path(tree, f, fused32, 0);
   PathSpec<float, float> a = f;
-  a.X = Y32.p; a.factor = false;
+  a.X = Y32.p; a.factor = false; a.factors = &fused32.leaf;
   build_path(tree, a, apply32, 0);
 }
 

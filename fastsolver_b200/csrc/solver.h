@@ -47,13 +47,12 @@ struct DevBuf {
 
 // Per-node factorization data kept for solves with the same factors.
 struct NodeStore {
-  DevBuf<double> S_lu;   // per node: s_slot doubles
-  DevBuf<double> S_inv;  // per node: s_slot doubles
-  DevBuf<double> ident;  // s_max x s_max identity (the I of S = I - V1Tu1 V0Tu0)
-  DevBuf<int> S_piv;     // per node: s_max ints
-  DevBuf<double> VTu0;   // per node: r*r
-  DevBuf<double> VTu1;
-  int s_slot = 0, s_max = 0, rr = 0;
+  DevBuf<double> S;      // form 0, per node: S = I - V1Tu1 V0Tu0 (r x r)
+  DevBuf<double> F;      // per node: r x r FP64 work of the factor kernel
+  DevBuf<double> ident;  // r x r identity (the I of S)
+  DevBuf<double> M64;    // per node: (2r)^2 solve matrix, FP64 path
+  DevBuf<float> M32;     // per node: (2r)^2 solve matrix, mixed path
+  int rr = 0, mm = 0;
 };
 
 template <typename T, typename TE>
@@ -68,7 +67,10 @@ struct LevelPlan {
   DevBuf<GemmSeg<T>> gram_segs;
   int n_gram = 0, gram_max = 0;
   DevBuf<NodeTask<T, TE>> node_tasks;
-  int n_nodes = 0, max_s = 0, max_rs = 0, max_c = 0;
+  int n_nodes = 0, max_s = 0, max_r = 0;
+  DevBuf<GemmItem<T, T>> ap_items;  // [eta0; eta1] = M [V0Td0; V1Td1] per node
+  DevBuf<GemmSeg<T>> ap_segs;
+  int n_ap = 0, ap_max_m = 0, ap_max_n = 0;
   DevBuf<GemmItem<T, T>> bc_items;
   DevBuf<GemmSeg<T>> bc_segs;
   int n_bc = 0, bc_max_m = 0, bc_max_n = 0;
@@ -98,6 +100,7 @@ struct LeafPlan {
   DevBuf<LeafFactorTask<T>> tasks;
   DevBuf<T> Linv, Uinv;
   DevBuf<int> swapflag;
+  std::vector<LeafFactorTask<T>> host_tasks;  // for apply plans with these factors
   int nleaf = 0, max_n = 0, laswp_cols = 0, nb = 0;
   struct Fwd {
     int k0, panel;
@@ -117,6 +120,8 @@ struct PathPlan {
   DevBuf<LeafTask<T>> leaf_tasks;
   int nleaf = 0, max_n = 0, max_nrhs = 0;
   LeafPlan<T> leaf;     // factor paths: the blocked leaf factorization
+  DevBuf<LeafFactorTask<T>> apply_tasks;  // apply paths: the factors' tasks on X
+  int apply_nb = 0, apply_max_n = 0, apply_max_cols = 0;
   std::vector<std::unique_ptr<LevelPlan<T, TE>>> levels;  // deepest first
 };
 

@@ -213,11 +213,13 @@ __device__ inline void stage_row(float *dst, int sw, const float *base, long lon
   }
 }
 
-template <int BN, typename TC>
+template <int BN, bool SWAP, typename TC>
 __global__ void __launch_bounds__(kThreadsP, 1)
     tc_gemm_persistent(const GemmItem<float, TC> *__restrict__ items,
                        const GemmSeg<float> *__restrict__ segs, int nitems, int mtiles,
-                       int ntn, float alpha, float beta, int trans, int swap) {
+                       int ntn, float alpha, float beta, int trans) {
+  static_assert(sizeof(TC) == 4, "the engine writes FP32 results");
+  constexpr bool swap = SWAP;
   constexpr int A_BYTES = BM * BK * 2;  // one of hi / lo
   constexpr int B_BYTES = BN * BK * 2;
   constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char *ring = smem;
   float *stg = reinterpret_cast<float *>(smem + kStagesP * STAGE_BYTES);
-  float *cst = stg + kStg * (STG_BYTES / 4);  // C tile staging, BN x 128
+  float *cst = stg + kStg * (STG_BYTES / 4);  // C tile staging, 128 x (BN + 4)
   __shared__ __align__(8) uint64_t full[kStagesP], empty[kStagesP], tfull[2], tempty[2], fin;
   __shared__ uint32_t tmem_sh;
   __shared__ volatile int abort_sh;
@@ -398,21 +400,70 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     // ------------------------------------------------------------ epilogue
     const int q = warp & 3;        // TMEM lane quarter of this warp
     const int rl = q * 32 + lane;  // row of the tile owned by this thread
+    const int ew = warp - 5;       // epilogue warp 0..3
     int acc = 0;
     uint32_t aphase = 0;
-    // C staging [col][128 rows]: each thread copies and reads only its row
+    // Cin staging.  Non-swapped tiles: cst[j * 128 + row] (column j of the
+    // tile, filled a whole column per warp instruction with 16-byte copies).
+    // Swapped tiles: cst[row * CSTR + j] (row = item column, contiguous in
+    // memory along j, filled by the row's owner with 16-byte copies).
+    constexpr int CSTR = BN + 4;
     auto issue_c = [&](const GemmItem<float, TC> &it, int m0, int n0, int Mu, int Nu) {
-      const int drow = m0 + rl;
-      if (it.Cin != nullptr && sizeof(TC) == 4) {
+      if (it.Cin != nullptr) {
         const float *cin = reinterpret_cast<const float *>(it.Cin);
-        for (int j = 0; j < BN; ++j) {
-          const int dcol = n0 + j;
-          const bool ok = drow < Mu && dcol < Nu;
-          const int gm = swap ? dcol : drow, gn = swap ? drow : dcol;
-          cpa4(cst + j * 128 + rl, ok ? cin + gm + (long long)gn * it.ldcin : cin, ok);
+        const long long ld = it.ldcin;
+        const bool vec = ((reinterpret_cast<uintptr_t>(cin) & 15) == 0) && ((ld & 3) == 0);
+        if (!SWAP) {
+          // lane covers rows m0 + 4 lane .. + 3 of column n0 + j
+          const int r4 = m0 + 4 * lane;
+          for (int j = ew; j < BN; j += 4) {
+            const int dcol = n0 + j;
+            float *dst = cst + j * 128 + 4 * lane;
+            const float *src = cin + r4 + (long long)dcol * ld;
+            if (vec && dcol < Nu && r4 + 4 <= Mu) {
+              cpa16(dst, src);
+            } else {
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const bool ok = dcol < Nu && r4 + u < Mu;
+                cpa4(dst + u, ok ? src + u : cin, ok);
+              }
+            }
+          }
+        } else {
+          // this thread's item column gn = m0 + rl, item rows n0 .. n0 + BN
+          const int gn = m0 + rl;
+          float *dst = cst + rl * CSTR;
+          const float *src = cin + n0 + (long long)gn * ld;
+          const bool rowok = gn < Mu;
+          for (int j = 0; j < BN; j += 4) {
+            if (vec && rowok && n0 + j + 4 <= Nu) {
+              cpa16(dst + j, src + j);
+            } else {
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const bool ok = rowok && n0 + j + u < Nu;
+                cpa4(dst + j + u, ok ? src + j + u : cin, ok);
+              }
+            }
+          }
         }
       }
       cpa_commit();
+    };
+    auto epi_sync = [&]() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); };
+    // barrier of the 128 epilogue threads returning the OR of `p` (uniform exit decisions)
+    auto epi_vote_or = [&](bool p) -> bool {
+      uint32_t r;
+      asm volatile(
+          "{\n\t.reg .pred pi, po;\n\t"
+          "setp.ne.u32 pi, %1, 0;\n\t"
+          "bar.red.or.pred po, 1, 128, pi;\n\t"
+          "selp.u32 %0, 1, 0, po;\n\t}\n"
+          : "=r"(r)
+          : "r"((uint32_t)p)
+          : "memory");
+      return r != 0;
     };
     int t = blockIdx.x;
     GemmItem<float, TC> it;
@@ -424,12 +475,20 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     };
     bool have = next_tile();
     if (have) issue_c(it, m0, n0, Mu, Nu);
-    while (have && !abort_sh) {
+    while (have) {  // `have` is uniform across the epilogue threads
       const bool has_k = kstages(it) > 0;
-      const int drow = m0 + rl;
-      if (!mbar_wait(&tfull[acc], aphase)) { abort_sh = 1; break; }
+      const float a_eff = has_k ? alpha : 0.f;
+      const bool has_c = it.Cin != nullptr;
+      const bool ok = mbar_wait(&tfull[acc], aphase);
+      cpa_wait<0>();  // this thread's Cin copies have landed
+      // one barrier: every thread's copies visible, one exit decision for all
+      if (epi_vote_or(!ok || abort_sh)) {
+        if (!ok) abort_sh = 1;
+        break;
+      }
       tc_fence_after();
-      cpa_wait<0>();  // this tile's C rows have landed
+      float *C = reinterpret_cast<float *>(it.C);
+      const long long ldc = it.ldc;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN && n0 + c0 < Nu; c0 += 16) {
         uint32_t r[16];
@@ -442,25 +501,55 @@ __global__ void __launch_bounds__(kThreadsP, 1)
               "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-        if (drow < Mu) {
+        const int ncols = min(16, Nu - n0 - c0);
+        if (!SWAP) {
+          const int drow = m0 + rl;
+          if (drow < Mu) {
+            float *cp = C + drow + (long long)(n0 + c0) * ldc;
+            const float *cs = cst + c0 * 128 + rl;
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int dcol = n0 + c0 + j;
-            if (dcol >= Nu) break;
-            const int gm = swap ? dcol : drow, gn = swap ? drow : dcol;
-            float v = has_k ? alpha * __uint_as_float(r[j]) : 0.f;
-            if (it.Cin) {
-              const float c = sizeof(TC) == 4 ? cst[(c0 + j) * 128 + rl]
-                                              : float(it.Cin[gm + (long long)gn * it.ldcin]);
-              v += beta * c;
+            for (int j = 0; j < 16; ++j) {
+              if (j < ncols) {
+                float v = a_eff * __uint_as_float(r[j]);
+                if (has_c) v += beta * cs[j * 128];
+                cp[(long long)j * ldc] = v;
+              }
             }
-            it.C[gm + (long long)gn * it.ldc] = TC(v);
+          }
+        } else {
+          const int gn = m0 + rl;
+          if (gn < Mu) {
+            float *cp = C + (n0 + c0) + (long long)gn * ldc;
+            const float *cs = cst + rl * CSTR + c0;
+            float v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = a_eff * __uint_as_float(r[j]);
+            if (has_c) {
+#pragma unroll
+              for (int j = 0; j < 16; j += 4) {
+                const float4 c4 = *reinterpret_cast<const float4 *>(cs + j);
+                v[j] += beta * c4.x;
+                v[j + 1] += beta * c4.y;
+                v[j + 2] += beta * c4.z;
+                v[j + 3] += beta * c4.w;
+              }
+            }
+            if (ncols == 16 && (reinterpret_cast<uintptr_t>(cp) & 15) == 0) {
+#pragma unroll
+              for (int j = 0; j < 16; j += 4)
+                *reinterpret_cast<float4 *>(cp + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+            } else {
+#pragma unroll
+              for (int j = 0; j < 16; ++j)
+                if (j < ncols) cp[j] = v[j];
+            }
           }
         }
       }
       tc_fence_before();
       mbar_arrive(&tempty[acc]);
       if (++acc == 2) { acc = 0; aphase ^= 1; }
+      epi_sync();  // every thread is done with cst before it is refilled
       t += gridDim.x;
       have = next_tile();
       if (have) issue_c(it, m0, n0, Mu, Nu);  // lands while the next tile is computed
@@ -475,15 +564,14 @@ __global__ void __launch_bounds__(kThreadsP, 1)
                  "r"(TMEM_COLS));
 }
 
-template <int BN, typename TC>
+template <int BN, bool SWAP, typename TC>
 void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int nitems,
-               int mu_max, int nu_max, bool trans, bool swap, float alpha, float beta,
-               cudaStream_t s) {
+               int mu_max, int nu_max, bool trans, float alpha, float beta, cudaStream_t s) {
   constexpr int STAGE_BYTES = 2 * BM * BK * 2 + 2 * BN * BK * 2;
   constexpr int STG_BYTES = 2 * 128 * BK * 4;
-  const size_t smem =
-      (size_t)kStagesP * STAGE_BYTES + (size_t)kStg * STG_BYTES + (size_t)BN * 128 * 4 + 128;
-  HODLR_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_persistent<BN, TC>,
+  const size_t smem = (size_t)kStagesP * STAGE_BYTES + (size_t)kStg * STG_BYTES +
+                      (size_t)(BN + 4) * 128 * 4 + 128;
+  HODLR_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_persistent<BN, SWAP, TC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int mt = cdiv(mu_max, BM), nt = cdiv(nu_max, BN);
   const long long total = (long long)nitems * mt * nt;
@@ -495,8 +583,8 @@ void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int
     cudaGetLastError();
   }
   const int grid = (int)std::min<long long>(total, sms);
-  tc_gemm_persistent<BN, TC><<<grid, kThreadsP, smem, s>>>(items, segs, nitems, mt, nt, alpha,
-                                                           beta, trans ? 1 : 0, swap ? 1 : 0);
+  tc_gemm_persistent<BN, SWAP, TC><<<grid, kThreadsP, smem, s>>>(items, segs, nitems, mt, nt,
+                                                                 alpha, beta, trans ? 1 : 0);
   HODLR_LAUNCH_CHECK();
 }
 
@@ -509,8 +597,13 @@ void launch_tc_gemm(const GemmItem<float, TC> *items, const GemmSeg<float> *segs
   // put the wider side on the UMMA M = 128 side
   const bool swap = max_m < 128 && max_n > max_m;
   const int mu = swap ? max_n : max_m, nu = swap ? max_m : max_n;
-  if (nu <= 64) launch_bn<64, TC>(items, segs, nitems, mu, nu, trans, swap, alpha, beta, s);
-  else launch_bn<128, TC>(items, segs, nitems, mu, nu, trans, swap, alpha, beta, s);
+  if (swap) {
+    if (nu <= 64) launch_bn<64, true, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+    else launch_bn<128, true, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+  } else {
+    if (nu <= 64) launch_bn<64, false, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+    else launch_bn<128, false, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+  }
 }
 
 int tc_error_flag(bool reset) {
