@@ -92,6 +92,39 @@ def phase_bytes(tree: np.ndarray, m: int, word: int):
     return b
 
 
+def leaf_update_bytes(tree: np.ndarray, word: int, nb: int = 64) -> float:
+    """Algorithmic bytes of all leaf trailing-update GEMMs of one factor pass:
+    per panel, C = A22|X (rest x (rest + ncols)) read and written, L21
+    (rest x kb) and U12 (kb x (rest + ncols)) read once."""
+    nrow, ncol, rb, cb, lc, rc, par, dep, vnc, leaf = (tree[:, i] for i in range(10))
+    tot = 0.0
+    for i in range(tree.shape[0]):
+        if not leaf[i]:
+            continue
+        n = int(nrow[i])
+        ncols = int(cb[i] + ncol[i])
+        for k0 in range(0, n, nb):
+            kb = min(nb, n - k0)
+            rest = n - k0 - kb
+            if rest <= 0:
+                continue
+            w = rest + ncols
+            tot += word * (2.0 * rest * w + rest * kb + kb * w)
+    return tot
+
+
+def profile_traffic(path: str):
+    """DRAM bytes per launch (read + write) recorded by an ncu capture summary."""
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
 # ---------------------------------------------------------------------------
 # clocks sampling during the timed region
 # ---------------------------------------------------------------------------
@@ -177,6 +210,22 @@ def dist_env():
     return ws, rank, local
 
 
+def rank_max(x: float, dist=None, device="cuda") -> float:
+    """Max of a per-rank scalar over all ranks (the timing rule: the slowest
+    rank defines the step time); identity without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ms_max: float, world_size: int) -> float:
+    """Whole-job solves/s of `world_size` replicas, each one solve per step."""
+    return world_size * 1e3 / ms_max
+
+
 def make_system(fs, cfg, seed):
     h = fs.HodlrMatrix(cfg["nrhs"], cfg["N"], cfg["rank"], cfg["leaf"]).create_tree()
     h.init_gaussian(seed, 0.5)
@@ -235,6 +284,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-solves", type=int, default=2)
+    ap.add_argument("--profile-one", choices=["mixed", "fp64"], default=None,
+                    help="warm up, then run one solve between cudaProfilerStart/Stop and exit "
+                         "(for ncu --profile-from-start off); prints no bench line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = CONFIGS[args.config]
@@ -257,11 +309,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, dist, "cuda")
 
     stream = torch.cuda.current_stream()
     h = make_system(fs, cfg, args.seed + rank)
@@ -274,6 +322,18 @@ def main():
 
     def fp64_step():
         solver.bfs_solve(h, sync=False, stream=stream)
+
+    if args.profile_one:
+        step = mixed_step if args.profile_one == "mixed" else fp64_step
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        step()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(f"profiled one {args.profile_one} solve of {args.config}", flush=True)
+        return
 
     # ---- warm-up
     for _ in range(args.warmup):
@@ -351,7 +411,7 @@ def main():
         torch.cuda.synchronize()
         ms_e2e = max_over_ranks(e0.elapsed_time(e1) / ksteps)
         h2d = (Dp.numel() + Up.numel() + Vp.numel() + Bp.numel()) * 8
-        e2e = {"value": ws * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": replica_value(ms_e2e, ws), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(xout.numel() * 8), "ms_per_step": ms_e2e,
                "steps": ksteps}
 
@@ -369,35 +429,36 @@ def main():
     B8 = phase_bytes(tree, m, 8)
     fp32_peak = simt_peak_tflops(4, pk["sm_mhz"])
     fp64_peak = simt_peak_tflops(8, pk["sm_mhz"])
-    phase_flops = {"getrf": W["getrf"], "getrs": W["getrs"], "reduce": W["reduce"],
-                   "node_apply": W["node"], "broadcast": W["broadcast"]}
-    # the factor pass of the mixed solve carries b, so its per-phase work equals the
-    # fused model; refinement sweeps add getrs/reduce/broadcast launches on m columns
-    dom = max(("getrf", "getrs", "reduce", "broadcast"),
-              key=lambda k: ph_mixed[k][0])
-    ms_dom, n_dom = ph_mixed[dom]
-    # the dominant phase's first launch is the factor pass: time one launch of it
+    # Dominant kernel: the leaf trailing updates A22 -= L21 U12 of the blocked
+    # FP32 leaf factorization (tcgen05 split-BF16 GEMM engine), HBM-bound at
+    # K = 64.  Algorithmic bytes per launch = read + write of the updated
+    # block plus both operands, FP32, averaged over the launches; duration =
+    # the CUDA-event time of those launches in one factor pass / launches.
     h.set_profiling(True)
     solver.factor(h, fs.PREC_MIXED, stream=stream)
     ph_f = h.phase_times(reset=True)
     h.set_profiling(False)
-    ms_one, n_one = ph_f[dom]
-    per_launch_ms = ms_one / max(n_one, 1)
-    flops_per_launch = phase_flops[dom] / (1 if dom in ("getrf", "getrs") else max(n_one, 1))
-    achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
-    roofline = {"bound": "fp32-simt", "kernel": {"getrf": "getrf_kernel<float>",
-                                                "getrs": "getrs_kernel<float>",
-                                                "reduce": "gemm_items_kernel<float> (reduce)",
-                                                "broadcast": "gemm_items_kernel<float> (bcast)"}[dom],
-                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp32_peak, "traffic": None,
-                "peak_note": f"nominal FP32 FMA peak 148 SM x 128 x 2 x {pk['sm_mhz']:.0f} MHz"}
+    ms_upd, n_upd = ph_f["leaf_update"]
+    upd_bytes = leaf_update_bytes(tree, 4)
+    per_launch_ms = ms_upd / max(n_upd, 1)
+    bytes_per_launch = upd_bytes / max(n_upd, 1)
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    traffic = profile_traffic(os.path.join(ROOT, "profiles", "leaf_update_gemm_n262144.md"))
+    roofline = {"bound": "hbm", "kernel": "tc_gemm_persistent<128,false> (leaf trailing update)",
+                "achieved": achieved, "peak": pk["hbm"], "unit": "GB/s",
+                "frac": achieved / pk["hbm"], "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "ms_per_launch": per_launch_ms, "launches": n_upd,
+                "peak_note": "measured HBM copy bandwidth of this pool's B200s"
+                             if pk["src"] == "measured" else "fallback 6650 GB/s"}
 
-    def solve_frac(ms, word, peak_tf):
+    def solve_frac(ms, word, peak_tf, passes=1):
+        """Roofline time of one fused solve / measured: every phase at the slower
+        of its flops (x passes: 3 for split-BF16) and its compulsory bytes."""
         Bx = B4 if word == 4 else B8
         t = 0.0
         for k in ("getrf", "getrs", "reduce", "broadcast"):
-            t += max(W[k] / (peak_tf * 1e12), Bx[k] / (pk["hbm"] * 1e9))
+            t += max(passes * W[k] / (peak_tf * 1e12), Bx[k] / (pk["hbm"] * 1e9))
         t += W["node"] / (fp64_peak * 1e12)
         return t * 1e3 / ms
 
@@ -418,7 +479,7 @@ def main():
                "sample": f"{args.cpu_solves} full fused FP64 solves of the same system "
                          "(oracle/refcpu.c, OpenBLAS, one OpenMP task per leaf/node)"}
 
-    value = ws * 1e3 / ms_mixed
+    value = replica_value(ms_mixed, ws)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
@@ -429,12 +490,12 @@ def main():
                    **cfg, "levels": int(tree[:, 7].max()), "l2": "inputs 3.5 GB > L2",
                    "parallelism": f"replicas x{ws}"},
         "relres_max": float(max(rrs)), "refine_sweeps": iters,
-        "fp64_gpu": {"value": ws * 1e3 / ms_fp64, "unit": "solves/s", "ms_per_step": ms_fp64,
+        "fp64_gpu": {"value": replica_value(ms_fp64, ws), "unit": "solves/s", "ms_per_step": ms_fp64,
                      "relres": rr_fp64,
                      "roofline_frac": solve_frac(ms_fp64, 8, fp64_peak),
                      "tflops": total_flops / (ms_fp64 * 1e-3) / 1e12},
         "mixed_over_fp64": ms_fp64 / ms_mixed,
-        "mixed_roofline_frac": solve_frac(ms_mixed, 4, fp32_peak),
+        "mixed_roofline_frac": solve_frac(ms_mixed, 4, pk["bf16"], passes=3),
         "gflop_per_solve": total_flops / 1e9,
         "roofline": roofline,
         "phases_ms": {"mixed": {k: round(v[0], 4) for k, v in ph_mixed.items()},

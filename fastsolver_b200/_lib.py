@@ -23,7 +23,7 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 
 PHASES = ["getrf", "getrs", "reduce", "node_factor", "node_apply", "broadcast", "matvec",
-          "convert"]
+          "convert", "leaf_panel", "leaf_update", "leaf_trsm"]
 NODE_FIELDS = ["nrow", "ncol", "row_beg", "col_beg", "lchild", "rchild", "parent", "depth",
                "vncol", "is_leaf"]
 

@@ -819,6 +819,8 @@ int hodlr_set_profiling(hodlr_system h, int on) {
   });
 }
 
+static_assert(PH_COUNT == HODLR_PHASES, "phase list of the C ABI");
+
 int hodlr_phase_times(hodlr_system h, double *ms, long long *launches, int reset) {
   if (!h) return -1;
   return guarded([&]() -> int {

@@ -441,10 +441,19 @@ void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t 
     PhaseScope ps(pf, PH_GETRF, s);
     launch_leaf_init<T>(lp.tasks.p, lp.nleaf, info, s);
     for (const auto &F : lp.fwd) {
-      launch_leaf_panel<T>(lp.tasks.p, lp.nleaf, lp.max_n, lp.nb, F->k0, F->panel, info, s);
-      launch_leaf_laswp<T>(lp.tasks.p, lp.nleaf, lp.laswp_cols, lp.nb, F->k0, F->panel, s);
-      run_gemm<T, T, T>(F->trsm, false, T(1), T(0), s);
-      run_gemm<T, T, T>(F->update, false, T(-1), T(1), s);
+      {
+        PhaseScope pp(pf, PH_LEAF_PANEL, s);
+        launch_leaf_panel<T>(lp.tasks.p, lp.nleaf, lp.max_n, lp.nb, F->k0, F->panel, info, s);
+        launch_leaf_laswp<T>(lp.tasks.p, lp.nleaf, lp.laswp_cols, lp.nb, F->k0, F->panel, s);
+      }
+      if (F->trsm.n > 0) {
+        PhaseScope pt(pf, PH_LEAF_TRSM, s);
+        run_gemm<T, T, T>(F->trsm, false, T(1), T(0), s);
+      }
+      if (F->update.n > 0) {
+        PhaseScope pu(pf, PH_LEAF_UPDATE, s);
+        run_gemm<T, T, T>(F->update, false, T(-1), T(1), s);
+      }
     }
   }
   {

@@ -142,7 +142,7 @@ struct MatvecPlan {
 // Optional per-phase timing (CUDA events around each launch group).
 enum Phase {
   PH_GETRF = 0, PH_GETRS, PH_REDUCE, PH_NODE_FACTOR, PH_NODE_APPLY, PH_BCAST, PH_MATVEC,
-  PH_CONVERT, PH_COUNT
+  PH_CONVERT, PH_LEAF_PANEL, PH_LEAF_UPDATE, PH_LEAF_TRSM, PH_COUNT
 };
 struct Profiler {
   bool on = false;

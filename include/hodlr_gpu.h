@@ -206,8 +206,10 @@ int hodlr_solve_fused(hodlr_system sys, int schur2, int sync,
                       hodlr_stream_t stream);
 
 /* Factor/solve split (no reference counterpart: the reference always fuses).
- * hodlr_factor keeps the leaf LU, the transformed U blocks and every node's
- * capacitance LU in `precision`; hodlr_solve applies them to the current RHS. */
+ * hodlr_factor keeps the leaf LU (with the inverses of its diagonal blocks),
+ * the transformed U blocks and every node's solve matrix M
+ * ([eta0; eta1] = M [V0Td0; V1Td1]) in `precision`; hodlr_solve applies
+ * them to the current RHS. */
 int hodlr_factor(hodlr_system sys, int precision, hodlr_stream_t stream);
 int hodlr_solve(hodlr_system sys, hodlr_stream_t stream);
 
@@ -236,9 +238,12 @@ int hodlr_get_solution(hodlr_system sys, double *X, long long ldx, int host,
  * launch group is bracketed by CUDA events; hodlr_phase_times synchronizes
  * and returns, per phase, the accumulated milliseconds and the number of
  * launches since the last reset (ms / launches: arrays of HODLR_PHASES,
- * either may be NULL).  Phases: 0 getrf, 1 getrs, 2 reduce, 3 node factor,
- * 4 node apply, 5 broadcast, 6 matvec, 7 precision conversion. */
-#define HODLR_PHASES 8
+ * either may be NULL).  Phases: 0 getrf (the forward blocked leaf
+ * factorization, all of 8-10), 1 getrs (backward leaf solve / leaf apply),
+ * 2 reduce, 3 node factor, 4 node apply, 5 broadcast, 6 matvec, 7 precision
+ * conversion, 8 leaf panels (panel LU + row interchanges), 9 leaf trailing
+ * updates (A22 -= L21 U12), 10 leaf panel solves (U12 = L11^{-1} A12). */
+#define HODLR_PHASES 11
 int hodlr_set_profiling(hodlr_system sys, int on);
 int hodlr_phase_times(hodlr_system sys, double *ms, long long *launches,
                       int reset);
