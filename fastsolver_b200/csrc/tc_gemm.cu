@@ -30,6 +30,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "gemm_simt.cuh"
 #include "tc_gemm.cuh"
 
 namespace hodlr {
@@ -122,20 +123,21 @@ __device__ inline uint32_t kmajor_off(int rows, int row, int kchunk_global) {
 }
 
 // Split 8 FP32 values into hi / lo bf16 and store one 16-byte chunk of each.
+// Pairs go through the packed conversion: hi = bf16x2(x), lo = bf16x2(x - hi).
 __device__ inline void split_store8(const float *v, unsigned char *hi, unsigned char *lo,
                                     uint32_t off) {
-  __nv_bfloat162 h[4], l[4];
+  uint32_t h[4], l[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const __nv_bfloat16 h0 = __float2bfloat16_rn(v[2 * q]);
-    const __nv_bfloat16 h1 = __float2bfloat16_rn(v[2 * q + 1]);
-    const __nv_bfloat16 l0 = __float2bfloat16_rn(v[2 * q] - __bfloat162float(h0));
-    const __nv_bfloat16 l1 = __float2bfloat16_rn(v[2 * q + 1] - __bfloat162float(h1));
-    h[q] = __halves2bfloat162(h0, h1);
-    l[q] = __halves2bfloat162(l0, l1);
+    const __nv_bfloat162 hb = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+    const uint32_t hu = *reinterpret_cast<const uint32_t *>(&hb);
+    const float h0 = __uint_as_float(hu << 16), h1 = __uint_as_float(hu & 0xffff0000u);
+    const __nv_bfloat162 lb = __floats2bfloat162_rn(v[2 * q] - h0, v[2 * q + 1] - h1);
+    h[q] = hu;
+    l[q] = *reinterpret_cast<const uint32_t *>(&lb);
   }
-  *reinterpret_cast<uint4 *>(hi + off) = *reinterpret_cast<const uint4 *>(h);
-  *reinterpret_cast<uint4 *>(lo + off) = *reinterpret_cast<const uint4 *>(l);
+  *reinterpret_cast<uint4 *>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4 *>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
 __device__ inline void mbar_arrive(uint64_t *bar) {
@@ -150,7 +152,8 @@ __device__ inline void mbar_arrive(uint64_t *bar) {
 //     stage into bf16 hi / lo and writes the UMMA K-major ring (full[s]:
 //     128 arrivals, empty[s]: tcgen05.commit).
 //   warp 4 lane 0 (MMA issuer): 3 MMAs per 16-deep k-step into one of two TMEM
-//     accumulators (tfull[a]: commit, tempty[a]: 128 epilogue arrivals).
+//     accumulators (tfull[a]: commit; tready[a]: 128 epilogue arrivals once
+//     the buffer is drained and preloaded with the next tile's scaled Cin).
 //   warps 5-8 (epilogue): thread r owns row r of the tile; it prefetches the
 //     next tile's C row with cp.async as soon as the current tile is drained,
 //     then drains TMEM 16 columns at a time: D = alpha * acc + beta * Cin.
@@ -186,29 +189,39 @@ struct KPos {
 // thread's own staging row) with cp.async; zero-filled outside the matrix.
 // The row's eight 16-byte chunks are XOR-swizzled by `sw` (= row & 7) so that
 // the 32 lanes reading their rows chunk by chunk hit distinct banks.
+__device__ inline void cpa4_u(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(dst)), "l"(src));
+}
 __device__ inline void stage_row(float *dst, int sw, const float *base, long long ld,
                                  bool kcontig, int row, int rows_valid, int k0, int K) {
-  auto slot = [&](int k) { return dst + ((((k >> 2) ^ sw) << 2) | (k & 3)); };
+  float *chunk[BK / 4];
+#pragma unroll
+  for (int g = 0; g < BK / 4; ++g) chunk[g] = dst + ((g ^ sw) << 2);
+  const bool inrow = row < rows_valid;
+  const bool full = inrow && k0 + BK <= K;
   if (kcontig) {
     const float *p = base + (long long)row * ld + k0;
-    const bool inrow = row < rows_valid;
-    if (inrow && k0 + BK <= K && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+    if (full && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
 #pragma unroll
-      for (int q = 0; q < BK / 4; ++q) cpa16(slot(4 * q), p + 4 * q);
+      for (int g = 0; g < BK / 4; ++g) cpa16(chunk[g], p + 4 * g);
     } else {
 #pragma unroll
       for (int k = 0; k < BK; ++k) {
         const bool ok = inrow && k0 + k < K;
-        cpa4(slot(k), ok ? p + k : base, ok);
+        cpa4(chunk[k >> 2] + (k & 3), ok ? p + k : base, ok);
       }
     }
   } else {
-    const bool inrow = row < rows_valid;
     const float *p = base + row + (long long)k0 * ld;
+    if (full) {
 #pragma unroll
-    for (int k = 0; k < BK; ++k) {
-      const bool ok = inrow && k0 + k < K;
-      cpa4(slot(k), ok ? p + (long long)k * ld : base, ok);
+      for (int k = 0; k < BK; ++k) cpa4_u(chunk[k >> 2] + (k & 3), p + (long long)k * ld);
+    } else {
+#pragma unroll
+      for (int k = 0; k < BK; ++k) {
+        const bool ok = inrow && k0 + k < K;
+        cpa4(chunk[k >> 2] + (k & 3), ok ? p + (long long)k * ld : base, ok);
+      }
     }
   }
 }
@@ -229,7 +242,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
   unsigned char *ring = smem;
   float *stg = reinterpret_cast<float *>(smem + kStagesP * STAGE_BYTES);
   float *cst = stg + kStg * (STG_BYTES / 4);  // C tile staging, 128 x (BN + 4)
-  __shared__ __align__(8) uint64_t full[kStagesP], empty[kStagesP], tfull[2], tempty[2], fin;
+  __shared__ __align__(8) uint64_t full[kStagesP], empty[kStagesP], tfull[2], tready[2], fin;
   __shared__ uint32_t tmem_sh;
   __shared__ volatile int abort_sh;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -242,7 +255,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&tfull[a], 1);
-      mbar_init(&tempty[a], 128);
+      mbar_init(&tready[a], 128);
     }
     mbar_init(&fin, 1);
     abort_sh = 0;
@@ -259,11 +272,21 @@ __global__ void __launch_bounds__(kThreadsP, 1)
   tc_fence_after();
   const uint32_t tmem = tmem_sh;
 
+  // t / d for t < 2^24 through a float reciprocal, corrected to the exact quotient
+  const int mn = mtiles * ntn;
+  const float inv_mn = 1.0f / float(mn), inv_n = 1.0f / float(ntn);
+  auto qdiv = [](int t, int d, float inv) {
+    int q = __float2int_rz(float(t) * inv);
+    if (q * d > t) --q;
+    else if ((q + 1) * d <= t) ++q;
+    return q;
+  };
   auto decode = [&](int t, GemmItem<float, TC> &it, int &m0, int &n0, int &Mu, int &Nu) {
-    const int item = t / (mtiles * ntn);
-    const int rem = t - item * (mtiles * ntn);
-    m0 = (rem / ntn) * BM;
-    n0 = (rem % ntn) * BN;
+    const int item = qdiv(t, mn, inv_mn);
+    const int rem = t - item * mn;
+    const int mt = qdiv(rem, ntn, inv_n);
+    m0 = mt * BM;
+    n0 = (rem - mt * ntn) * BN;
     it = items[item];
     Mu = swap ? it.N : it.M;
     Nu = swap ? it.M : it.N;
@@ -368,10 +391,13 @@ __global__ void __launch_bounds__(kThreadsP, 1)
         GemmItem<float, TC> it;
         int m0, n0, Mu, Nu;
         if (!decode(t, it, m0, n0, Mu, Nu)) continue;
-        if (!mbar_wait(&tempty[acc], aphase ^ 1)) { abort_sh = 1; break; }
+        // the epilogue has drained this accumulator and preloaded it with
+        // (beta / alpha) Cin when the item has one
+        if (!mbar_wait(&tready[acc], aphase)) { abort_sh = 1; break; }
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(acc * BN);
         const int nst = kstages(it);
+        const uint32_t pre = (it.Cin != nullptr && beta != 0.f) ? 1u : 0u;
         for (int ks_all = 0; ks_all < nst; ++ks_all) {
           if (!mbar_wait(&full[stage], phase)) { abort_sh = 1; break; }
           tc_fence_after();
@@ -382,7 +408,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
             const uint32_t ao = ks * (BM / 8) * 256, bo = ks * (BN / 8) * 256;
             const uint64_t dah = smem_desc(a_hi + ao, 128, 256), dal = smem_desc(a_lo + ao, 128, 256);
             const uint64_t dbh = smem_desc(b_hi + bo, 128, 256), dbl = smem_desc(b_lo + bo, 128, 256);
-            mma_bf16(d, dah, dbh, idesc, (ks_all > 0 || ks > 0) ? 1u : 0u);
+            mma_bf16(d, dah, dbh, idesc, (ks_all > 0 || ks > 0) ? 1u : pre);
             mma_bf16(d, dah, dbl, idesc, 1u);
             mma_bf16(d, dal, dbh, idesc, 1u);
           }
@@ -465,22 +491,92 @@ __global__ void __launch_bounds__(kThreadsP, 1)
           : "memory");
       return r != 0;
     };
-    int t = blockIdx.x;
-    GemmItem<float, TC> it;
-    int m0 = 0, n0 = 0, Mu = 0, Nu = 0;
-    auto next_tile = [&]() {
-      for (; t < total; t += gridDim.x)
-        if (decode(t, it, m0, n0, Mu, Nu)) return true;
-      return false;
+    const float cscale = beta / alpha;  // alpha != 0 (launch_tc_gemm routes alpha = 0 away)
+    // The epilogue's tile sequence: tile j uses accumulator j & 1.  After
+    // tile j is drained, its buffer is preloaded with tile j + 2's
+    // (beta / alpha) Cin from the staging buffer (filled by cp.async while
+    // tile j + 1 was computed) and released to the MMA issuer, which then
+    // accumulates alpha^{-1}-scaled products onto it; the drain multiplies by
+    // alpha.
+    struct Tile {
+      GemmItem<float, TC> it;
+      int m0, n0, Mu, Nu;
+      bool valid;
     };
-    bool have = next_tile();
-    if (have) issue_c(it, m0, n0, Mu, Nu);
-    while (have) {  // `have` is uniform across the epilogue threads
-      const bool has_k = kstages(it) > 0;
-      const float a_eff = has_k ? alpha : 0.f;
-      const bool has_c = it.Cin != nullptr;
+    int tnext = blockIdx.x;
+    auto fetch = [&](Tile &T) {
+      T.valid = false;
+      for (; tnext < total; tnext += gridDim.x)
+        if (decode(tnext, T.it, T.m0, T.n0, T.Mu, T.Nu)) {
+          T.valid = true;
+          tnext += gridDim.x;
+          return;
+        }
+    };
+    // staged Cin (landed, visible to all epilogue threads) -> TMEM buffer b
+    auto preload = [&](const Tile &T, int b) {
+      if (!(T.it.Cin != nullptr && beta != 0.f)) return;
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        uint32_t r[16];
+        if (!SWAP) {
+          const float *cs = cst + c0 * 128 + rl;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) r[j] = __float_as_uint(cscale * cs[j * 128]);
+        } else {
+          const float *cs = cst + rl * CSTR + c0;
+#pragma unroll
+          for (int j = 0; j < 16; j += 4) {
+            const float4 c4 = *reinterpret_cast<const float4 *>(cs + j);
+            r[j] = __float_as_uint(cscale * c4.x);
+            r[j + 1] = __float_as_uint(cscale * c4.y);
+            r[j + 2] = __float_as_uint(cscale * c4.z);
+            r[j + 3] = __float_as_uint(cscale * c4.w);
+          }
+        }
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0);
+        asm volatile(
+            "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, "
+            "%10, %11, %12, %13, %14, %15, %16};\n" ::"r"(taddr),
+            "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
+            "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]),
+            "r"(r[14]), "r"(r[15]));
+      }
+      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+    };
+    auto release = [&](int b) {
+      tc_fence_before();
+      mbar_arrive(&tready[b]);
+    };
+    Tile cur, n1, n2;
+    fetch(cur);
+    fetch(n1);
+    fetch(n2);
+    // prologue: the first two tiles' buffers (uniform across the epilogue threads)
+    if (cur.valid) {
+      issue_c(cur.it, cur.m0, cur.n0, cur.Mu, cur.Nu);
+      cpa_wait<0>();
+      epi_sync();
+      preload(cur, 0);
+      epi_sync();  // staging free again
+      release(0);
+    }
+    if (n1.valid) {
+      issue_c(n1.it, n1.m0, n1.n0, n1.Mu, n1.Nu);
+      cpa_wait<0>();
+      epi_sync();
+      preload(n1, 1);
+      epi_sync();
+      release(1);
+    }
+    if (n2.valid) issue_c(n2.it, n2.m0, n2.n0, n2.Mu, n2.Nu);
+    else cpa_commit();
+    while (cur.valid) {  // the tile sequence is uniform across the epilogue threads
+      const GemmItem<float, TC> &it = cur.it;
+      const int m0 = cur.m0, n0 = cur.n0, Mu = cur.Mu, Nu = cur.Nu;
+      const bool live = kstages(it) > 0 || (it.Cin != nullptr && beta != 0.f);
       const bool ok = mbar_wait(&tfull[acc], aphase);
-      cpa_wait<0>();  // this thread's Cin copies have landed
+      cpa_wait<0>();  // tile j + 2's Cin staged by this thread
       // one barrier: every thread's copies visible, one exit decision for all
       if (epi_vote_or(!ok || abort_sh)) {
         if (!ok) abort_sh = 1;
@@ -489,6 +585,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       tc_fence_after();
       float *C = reinterpret_cast<float *>(it.C);
       const long long ldc = it.ldc;
+      const float a_eff = live ? alpha : 0.f;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN && n0 + c0 < Nu; c0 += 16) {
         uint32_t r[16];
@@ -506,53 +603,38 @@ __global__ void __launch_bounds__(kThreadsP, 1)
           const int drow = m0 + rl;
           if (drow < Mu) {
             float *cp = C + drow + (long long)(n0 + c0) * ldc;
-            const float *cs = cst + c0 * 128 + rl;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              if (j < ncols) {
-                float v = a_eff * __uint_as_float(r[j]);
-                if (has_c) v += beta * cs[j * 128];
-                cp[(long long)j * ldc] = v;
-              }
-            }
+            for (int j = 0; j < 16; ++j)
+              if (j < ncols) cp[(long long)j * ldc] = a_eff * __uint_as_float(r[j]);
           }
         } else {
           const int gn = m0 + rl;
           if (gn < Mu) {
             float *cp = C + (n0 + c0) + (long long)gn * ldc;
-            const float *cs = cst + rl * CSTR + c0;
-            float v[16];
-#pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = a_eff * __uint_as_float(r[j]);
-            if (has_c) {
-#pragma unroll
-              for (int j = 0; j < 16; j += 4) {
-                const float4 c4 = *reinterpret_cast<const float4 *>(cs + j);
-                v[j] += beta * c4.x;
-                v[j + 1] += beta * c4.y;
-                v[j + 2] += beta * c4.z;
-                v[j + 3] += beta * c4.w;
-              }
-            }
             if (ncols == 16 && (reinterpret_cast<uintptr_t>(cp) & 15) == 0) {
 #pragma unroll
               for (int j = 0; j < 16; j += 4)
-                *reinterpret_cast<float4 *>(cp + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                *reinterpret_cast<float4 *>(cp + j) =
+                    make_float4(a_eff * __uint_as_float(r[j]), a_eff * __uint_as_float(r[j + 1]),
+                                a_eff * __uint_as_float(r[j + 2]), a_eff * __uint_as_float(r[j + 3]));
             } else {
 #pragma unroll
               for (int j = 0; j < 16; ++j)
-                if (j < ncols) cp[j] = v[j];
+                if (j < ncols) cp[j] = a_eff * __uint_as_float(r[j]);
             }
           }
         }
       }
-      tc_fence_before();
-      mbar_arrive(&tempty[acc]);
+      // buffer `acc` now belongs to tile j + 2: preload its Cin and release it
+      if (n2.valid) preload(n2, acc);
+      epi_sync();  // staging free for tile j + 3
+      release(acc);
       if (++acc == 2) { acc = 0; aphase ^= 1; }
-      epi_sync();  // every thread is done with cst before it is refilled
-      t += gridDim.x;
-      have = next_tile();
-      if (have) issue_c(it, m0, n0, Mu, Nu);  // lands while the next tile is computed
+      cur = n1;
+      n1 = n2;
+      fetch(n2);
+      if (n2.valid) issue_c(n2.it, n2.m0, n2.n0, n2.Mu, n2.Nu);
+      else cpa_commit();
     }
     cpa_wait<0>();
   }
@@ -594,6 +676,13 @@ template <typename TC>
 void launch_tc_gemm(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int nitems,
                     int max_m, int max_n, bool trans, float alpha, float beta, cudaStream_t s) {
   if (nitems <= 0 || max_m <= 0 || max_n <= 0) return;
+  if (alpha == 0.f) {
+    // C = beta Cin: the engine folds Cin into the accumulator as (beta / alpha) Cin
+    launch_gemm_items<float, float, float>(reinterpret_cast<const GemmItem<float, float> *>(items),
+                                           segs, nitems, max_m, max_n, trans, alpha, beta, s,
+                                           false);
+    return;
+  }
   // put the wider side on the UMMA M = 128 side
   const bool swap = max_m < 128 && max_n > max_m;
   const int mu = swap ? max_n : max_m, nu = swap ? max_m : max_n;
