@@ -40,7 +40,17 @@ __device__ int g_tc_error = 0;
 namespace {
 
 constexpr int BM = 128;    // UMMA M
-constexpr int BK = 32;     // K per stage (two MMA k-steps of 16)
+// Operand split.  BF16 (kind::f16, the default): hi = bf16(x), lo = bf16(x - hi),
+// each product accurate to ~2^-16 relative.  TF32 (kind::tf32, compile-time
+// alternative): hi = tf32(x), lo = tf32(x - hi), ~2^-21.  Both keep 64 bytes
+// of K per operand row and stage (two MMA k-steps), so the canonical smem
+// layout is the same.  Measured at N = 262144 (r = 64, m = 16): both need
+// two FP64 refinement sweeps to reach 1e-12 (after one sweep 2.8e-11 with
+// TF32, 9.6e-13 with plain FP32 FMA), so the cheaper BF16 split is used.
+constexpr bool kTF32 = false;
+constexpr int ELEM = kTF32 ? 4 : 2;  // bytes per split operand element
+constexpr int BK = 64 / ELEM;        // K per stage
+constexpr int MMA_K = 32 / ELEM;     // K per tcgen05.mma
 constexpr long long kSpinLimit = 1LL << 26;
 
 __device__ inline uint32_t smem_u32(const void *p) {
@@ -89,11 +99,12 @@ __device__ inline uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t
   return d;
 }
 
-// Instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major.
+// Instruction descriptor: kind::tf32 (A = B = TF32) or kind::f16 (A = B =
+// BF16), D = F32, both K-major.
 __host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
   return (1u << 4)                       // D format F32
-         | (1u << 7)                     // A format BF16
-         | (1u << 10)                    // B format BF16
+         | ((kTF32 ? 2u : 1u) << 7)      // A format
+         | ((kTF32 ? 2u : 1u) << 10)     // B format
          | ((uint32_t)(N >> 3) << 17)    // N
          | ((uint32_t)(M >> 4) << 24);   // M
 }
@@ -101,12 +112,21 @@ __host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
 __device__ inline void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
                                 uint32_t accumulate) {
   const uint32_t z = 0;  // disable-output-lane mask: all lanes written
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-          tmem_d),
-      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+  if constexpr (kTF32) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+            tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+            tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+  }
 }
 
 __device__ inline void mma_commit(uint64_t *bar) {
@@ -116,7 +136,7 @@ __device__ inline void mma_commit(uint64_t *bar) {
 }
 
 // Canonical K-major offset (bytes) of element (row, k) inside one operand
-// stage holding `rows` rows x BK k: [kstep][row/8][k-chunk][row%8][8 elems].
+// stage holding `rows` rows x BK k: [kstep][row/8][k-chunk][row%8][16 bytes].
 __device__ inline uint32_t kmajor_off(int rows, int row, int kchunk_global) {
   const int ks = kchunk_global >> 1, kc = kchunk_global & 1;
   return (uint32_t)(ks * (rows / 8) * 256 + (row >> 3) * 256 + kc * 128 + (row & 7) * 16);
@@ -140,6 +160,27 @@ __device__ inline void split_store8(const float *v, unsigned char *hi, unsigned 
   *reinterpret_cast<uint4 *>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// Split 4 FP32 values into hi / lo tf32 and store one 16-byte chunk of each.
+__device__ inline void split_store4_tf32(const float *v, unsigned char *hi, unsigned char *lo,
+                                         uint32_t off) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h[q]) : "f"(v[q]));
+    const float r = v[q] - __uint_as_float(h[q]);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l[q]) : "f"(r));
+  }
+  *reinterpret_cast<uint4 *>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4 *>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// One 16-byte chunk (16 / ELEM values) of each split operand.
+__device__ inline void split_chunk(const float *v, unsigned char *hi, unsigned char *lo,
+                                   uint32_t off) {
+  if constexpr (kTF32) split_store4_tf32(v, hi, lo, off);
+  else split_store8(v, hi, lo, off);
+}
+
 __device__ inline void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -159,8 +200,8 @@ __device__ inline void mbar_arrive(uint64_t *bar) {
 //     then drains TMEM 16 columns at a time: D = alpha * acc + beta * Cin.
 constexpr int kWarps = 9;
 constexpr int kThreadsP = kWarps * 32;
-constexpr int kStagesP = 2;  // UMMA operand ring
-constexpr int kStg = 3;      // FP32 staging ring (stages in flight per producer)
+constexpr int kStagesP = kTF32 ? 3 : 2;  // UMMA operand ring
+constexpr int kStg = kTF32 ? 4 : 3;      // FP32 staging ring (stages in flight per producer)
 
 __device__ inline void cpa4(void *dst, const void *src, bool ok) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
@@ -233,8 +274,8 @@ __global__ void __launch_bounds__(kThreadsP, 1)
                        int ntn, float alpha, float beta, int trans) {
   static_assert(sizeof(TC) == 4, "the engine writes FP32 results");
   constexpr bool swap = SWAP;
-  constexpr int A_BYTES = BM * BK * 2;  // one of hi / lo
-  constexpr int B_BYTES = BN * BK * 2;
+  constexpr int A_BYTES = BM * BK * ELEM;  // one of hi / lo
+  constexpr int B_BYTES = BN * BK * ELEM;
   constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   constexpr int STG_BYTES = 2 * 128 * BK * 4;  // A and B rows of the 128 producers
   constexpr int TMEM_COLS = 2 * BN;
@@ -332,7 +373,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       float *b = a + 128 * BK;
       if (ps.valid) {
         const GemmSeg<float> &sg = ps.sg;
-        const int sw = p & 7;
+        const int sw = kTF32 ? ((p >> 1) & 3) : (p & 7);
         if (!swap) {
           stage_row(a, sw, sg.A, sg.lda, trans != 0, ps.m0 + p, ps.it.M, ps.k0, sg.K);
           stage_row(b, sw, sg.B, sg.ldb, true, ps.n0 + p, p < BN ? ps.it.N : -1, ps.k0, sg.K);
@@ -358,7 +399,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       float va[BK], vb[BK];
 #pragma unroll
       for (int q = 0; q < BK / 4; ++q) {
-        const int qs = q ^ (p & 7);
+        const int qs = q ^ (kTF32 ? ((p >> 1) & 3) : (p & 7));
         const float4 x = reinterpret_cast<const float4 *>(a)[qs];
         const float4 y = reinterpret_cast<const float4 *>(b)[qs];
         va[4 * q] = x.x; va[4 * q + 1] = x.y; va[4 * q + 2] = x.z; va[4 * q + 3] = x.w;
@@ -370,10 +411,12 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       unsigned char *ahi = base, *alo = base + A_BYTES;
       unsigned char *bhi = base + 2 * A_BYTES, *blo = bhi + B_BYTES;
 #pragma unroll
-      for (int c = 0; c < BK / 8; ++c) split_store8(va + 8 * c, ahi, alo, kmajor_off(BM, p, c));
+      for (int c = 0; c < 4; ++c)
+        split_chunk(va + (16 / ELEM) * c, ahi, alo, kmajor_off(BM, p, c));
       if (p < BN) {
 #pragma unroll
-        for (int c = 0; c < BK / 8; ++c) split_store8(vb + 8 * c, bhi, blo, kmajor_off(BN, p, c));
+        for (int c = 0; c < 4; ++c)
+          split_chunk(vb + (16 / ELEM) * c, bhi, blo, kmajor_off(BN, p, c));
       }
       fence_proxy_async();
       mbar_arrive(&full[stage]);
@@ -404,7 +447,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
           const uint32_t a_hi = smem_u32(ring + stage * STAGE_BYTES), a_lo = a_hi + A_BYTES;
           const uint32_t b_hi = a_hi + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
 #pragma unroll
-          for (int ks = 0; ks < BK / 16; ++ks) {
+          for (int ks = 0; ks < BK / MMA_K; ++ks) {
             const uint32_t ao = ks * (BM / 8) * 256, bo = ks * (BN / 8) * 256;
             const uint64_t dah = smem_desc(a_hi + ao, 128, 256), dal = smem_desc(a_lo + ao, 128, 256);
             const uint64_t dbh = smem_desc(b_hi + bo, 128, 256), dbl = smem_desc(b_lo + bo, 128, 256);
@@ -649,7 +692,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
 template <int BN, bool SWAP, typename TC>
 void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int nitems,
                int mu_max, int nu_max, bool trans, float alpha, float beta, cudaStream_t s) {
-  constexpr int STAGE_BYTES = 2 * BM * BK * 2 + 2 * BN * BK * 2;
+  constexpr int STAGE_BYTES = 2 * BM * BK * ELEM + 2 * BN * BK * ELEM;
   constexpr int STG_BYTES = 2 * 128 * BK * 4;
   const size_t smem = (size_t)kStagesP * STAGE_BYTES + (size_t)kStg * STG_BYTES +
                       (size_t)(BN + 4) * 128 * 4 + 128;

@@ -1,8 +1,9 @@
 """The FP32 GEMM engines against a float64 torch reference.
 
-engine 0 is the FP32 FMA pipe; engine 1 the tcgen05 split-BF16 tensor-core
-kernel (three BF16 products, FP32 accumulation), whose relative error is
-bounded by a few 2^-16 of |A||B| -- the tolerance below.
+engine 0 is the FP32 FMA pipe; engine 1 the tcgen05 split-operand tensor-core
+kernel (x = hi + lo in BF16, three products hi*hi + hi*lo + lo*hi, FP32
+accumulation in tensor memory), whose relative error is bounded by a few
+2^-16 of |A||B| -- the tolerance below.
 """
 import numpy as np
 import pytest
@@ -36,10 +37,21 @@ SHAPES = [(128, 128, 32, 0), (448, 592, 64, 0), (64, 592, 64, 0), (512, 528, 64,
           (64, 592, 2048, 1), (64, 80, 4096, 1), (200, 300, 77, 0), (37, 45, 19, 1)]
 
 
+TC_TOL = 6e-5   # a few 2^-16 of |A||B|
+
+
 @pytest.mark.parametrize("m,n,k,transa", SHAPES)
-def test_tc_split_bf16_gemm(fs, cuda, m, n, k, transa):
+def test_tc_split_gemm(fs, cuda, m, n, k, transa):
     err = _run(1, transa, m, n, k, alpha=-1.0, beta=1.0, seed=m + n + k)
-    assert err < 6e-5, err   # a few 2^-16 of |A||B|
+    assert err < TC_TOL, err
+
+
+@pytest.mark.parametrize("alpha,beta", [(0.5, 2.0), (2.0, 0.0), (0.0, 3.0), (-1.5, -0.25)])
+def test_tc_split_gemm_scalars(fs, cuda, alpha, beta):
+    # the engine folds Cin into the accumulator as (beta / alpha) Cin
+    for m, n, k, transa in [(448, 592, 64, 0), (64, 592, 128, 1)]:
+        err = _run(1, transa, m, n, k, alpha=alpha, beta=beta, seed=m + k)
+        assert err < TC_TOL, (m, n, k, alpha, beta, err)
 
 
 @pytest.mark.parametrize("m,n,k,transa", SHAPES[:4])
