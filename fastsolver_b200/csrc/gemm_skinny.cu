@@ -8,13 +8,13 @@
 // (16-byte copies where the addresses allow) and compute from shared memory.
 //
 //   skinny_nn2: C (M x N) = beta Cin + alpha sum_s A_s B_s, A_s M x K column-
-//               major.  CTA = 256 rows of one item, thread = row, NC
-//               accumulators; per K tile the A tile (KT x 256) and the B tile
+//               major.  CTA = 512 rows of one item, thread = 2 rows, 2 x NC
+//               accumulators; per K tile the A tile (KT x 512) and the B tile
 //               (KT x NC) land in shared memory.
 //   skinny_tn2: C (M x N) = beta Cin + alpha sum_s A_s^T B_s, A_s K x M.
-//               CTA = 64 x 16 block of C of one item over all of K; thread
-//               (m, 4 columns), the A and B tiles stored k-contiguous so each
-//               thread reads 16-byte vectors along k.
+//               CTA (128 threads) = 64 x 16 block of C of one item over all
+//               of K; thread = rows (m, m + 32) x 4 columns, the A and B tiles
+//               stored k-contiguous so each thread reads 16-byte vectors along k.
 #include "common.cuh"
 #include "gemm_skinny.cuh"
 
@@ -78,12 +78,18 @@ struct Vec {
 };
 
 // ---------------------------------------------------------------- NN
+// CTA = 512 rows of one item, thread = rows (r, r + 256), 2 x NC accumulators,
+// so every broadcast read of B feeds two rows.
+constexpr int kNNRows = 2 * kSkThreads;
+template <typename T>
+__host__ __device__ constexpr int nn_kt() { return sizeof(T) == 4 ? 16 : 8; }
+
 template <typename T, int NC>
 __global__ void __launch_bounds__(kSkThreads)
     skinny_nn2_kernel(const GemmItem<T, T> *__restrict__ items, const GemmSeg<T> *__restrict__ segs,
                       T alpha, T beta) {
-  constexpr int KT = sizeof(T) == 4 ? 32 : 16;
-  constexpr int ROWS = kSkThreads;
+  constexpr int KT = nn_kt<T>();
+  constexpr int ROWS = kNNRows;
   constexpr int VW = Vec<T>::W;
   using V = typename Vec<T>::V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -93,7 +99,6 @@ __global__ void __launch_bounds__(kSkThreads)
   const int row0 = blockIdx.y * ROWS;
   if (row0 >= it.M) return;
   const int tid = threadIdx.x;
-  const int row = row0 + tid;
   const int N = it.N;
 
   auto load = [&](const TileIter<T> &p, int st) {
@@ -104,25 +109,26 @@ __global__ void __launch_bounds__(kSkThreads)
       const T *abase = sg.A + row0 + (long long)p.k0 * sg.lda;
       const bool vec = ((reinterpret_cast<uintptr_t>(abase) & 15) == 0) && ((sg.lda % VW) == 0);
       if (vec) {
-        // KT x (ROWS / VW) vectors
         for (int e = tid; e < KT * (ROWS / VW); e += kSkThreads) {
           const int k = e / (ROWS / VW), rv = e % (ROWS / VW);
           const int r = row0 + rv * VW;
-          const bool ok = (p.k0 + k < sg.K) && (r + VW <= it.M);
+          const bool kin = p.k0 + k < sg.K;
           const T *src = abase + rv * VW + (long long)k * sg.lda;
-          if (ok || r >= it.M || p.k0 + k >= sg.K) {
-            cpa(a + k * ROWS + rv * VW, ok ? src : sg.A, 16, ok);
+          if (kin && r + VW <= it.M) {
+            cpa(a + k * ROWS + rv * VW, src, 16, true);
           } else {
 #pragma unroll
-            for (int u = 0; u < VW; ++u)
-              cpa(a + k * ROWS + rv * VW + u, r + u < it.M ? src + u : sg.A, sizeof(T),
-                  r + u < it.M);
+            for (int u = 0; u < VW; ++u) {
+              const bool ok = kin && r + u < it.M;
+              cpa(a + k * ROWS + rv * VW + u, ok ? src + u : sg.A, sizeof(T), ok);
+            }
           }
         }
       } else {
-        for (int k = 0; k < KT; ++k) {
-          const bool ok = (p.k0 + k < sg.K) && row < it.M;
-          cpa(a + k * ROWS + tid, ok ? abase + tid + (long long)k * sg.lda : sg.A, sizeof(T), ok);
+        for (int e = tid; e < KT * ROWS; e += kSkThreads) {
+          const int k = e / ROWS, rr = e % ROWS;
+          const bool ok = (p.k0 + k < sg.K) && row0 + rr < it.M;
+          cpa(a + k * ROWS + rr, ok ? abase + rr + (long long)k * sg.lda : sg.A, sizeof(T), ok);
         }
       }
       for (int e = tid; e < KT * NC; e += kSkThreads) {
@@ -134,9 +140,9 @@ __global__ void __launch_bounds__(kSkThreads)
     cpa_commit();
   };
 
-  T acc[NC];
+  T acc0[NC], acc1[NC];
 #pragma unroll
-  for (int n = 0; n < NC; ++n) acc[n] = T(0);
+  for (int n = 0; n < NC; ++n) { acc0[n] = T(0); acc1[n] = T(0); }
   TileIter<T> ld, cp;
   ld.init(segs, it.seg_begin, it.seg_count);
   cp = ld;
@@ -154,15 +160,18 @@ __global__ void __launch_bounds__(kSkThreads)
     __syncthreads();
     const T *a = As + (size_t)st * KT * ROWS + tid;
     const T *b = Bs + (size_t)st * KT * NC;
-#pragma unroll 8
+#pragma unroll
     for (int k = 0; k < KT; ++k) {
-      const T av = a[k * ROWS];
+      const T a0 = a[k * ROWS], a1 = a[k * ROWS + kSkThreads];
 #pragma unroll
       for (int n = 0; n < NC; n += VW) {
         const V bv = *reinterpret_cast<const V *>(b + k * NC + n);
         const T *bp = reinterpret_cast<const T *>(&bv);
 #pragma unroll
-        for (int u = 0; u < VW; ++u) acc[n + u] += av * bp[u];
+        for (int u = 0; u < VW; ++u) {
+          acc0[n + u] += a0 * bp[u];
+          acc1[n + u] += a1 * bp[u];
+        }
       }
     }
     __syncthreads();  // stage st is refilled kSkStages - 1 tiles later
@@ -170,20 +179,26 @@ __global__ void __launch_bounds__(kSkThreads)
     cp.next(KT);
   }
   cpa_wait<0>();
-  if (row < it.M) {
 #pragma unroll
-    for (int n = 0; n < NC; ++n) {
-      if (n >= N) break;
-      T v = alpha * acc[n];
-      if (it.Cin) v += beta * it.Cin[row + (long long)n * it.ldcin];
-      it.C[row + (long long)n * it.ldc] = v;
+  for (int h = 0; h < 2; ++h) {
+    const int row = row0 + tid + h * kSkThreads;
+    if (row < it.M) {
+#pragma unroll
+      for (int n = 0; n < NC; ++n) {
+        if (n >= N) break;
+        T v = alpha * (h ? acc1[n] : acc0[n]);
+        if (it.Cin) v += beta * it.Cin[row + (long long)n * it.ldcin];
+        it.C[row + (long long)n * it.ldc] = v;
+      }
     }
   }
 }
 
 // ---------------------------------------------------------------- TN
+constexpr int kTNThreads = 128;
+
 template <typename T>
-__global__ void __launch_bounds__(kSkThreads)
+__global__ void __launch_bounds__(kTNThreads)
     skinny_tn2_kernel(const GemmItem<T, T> *__restrict__ items, const GemmSeg<T> *__restrict__ segs,
                       T alpha, T beta) {
   constexpr int TM = 64, TN = 16, KC = 32;
@@ -197,7 +212,7 @@ __global__ void __launch_bounds__(kSkThreads)
   const int m0 = blockIdx.y * TM, n0 = blockIdx.z * TN;
   if (m0 >= it.M || n0 >= it.N) return;
   const int tid = threadIdx.x;
-  const int mm = tid & (TM - 1), n4 = (tid >> 6) * 4;
+  const int mm = tid & 31, n4 = (tid >> 5) * 4;  // rows mm, mm + 32; columns n4 .. n4 + 3
 
   // rows (k) of a K x cols operand block, k-contiguous, into dst[col][LDK]
   auto load_block = [&](T *dst, const T *base, long long ld, int k0, int K, int c0, int ncols,
@@ -205,7 +220,7 @@ __global__ void __launch_bounds__(kSkThreads)
     const T *p0 = base + k0 + (long long)c0 * ld;
     const bool vec = ((reinterpret_cast<uintptr_t>(p0) & 15) == 0) && ((ld % VW) == 0);
     if (vec) {
-      for (int e = tid; e < ncols * (KC / VW); e += kSkThreads) {
+      for (int e = tid; e < ncols * (KC / VW); e += kTNThreads) {
         const int c = e / (KC / VW), kv = e % (KC / VW);
         const int k = k0 + kv * VW;
         const bool colok = c0 + c < cmax;
@@ -221,7 +236,7 @@ __global__ void __launch_bounds__(kSkThreads)
         }
       }
     } else {
-      for (int e = tid; e < ncols * KC; e += kSkThreads) {
+      for (int e = tid; e < ncols * KC; e += kTNThreads) {
         const int c = e / KC, kk = e % KC;
         const bool ok = c0 + c < cmax && k0 + kk < K;
         cpa(dst + c * LDK + kk, ok ? p0 + kk + (long long)c * ld : base, sizeof(T), ok);
@@ -236,7 +251,7 @@ __global__ void __launch_bounds__(kSkThreads)
     cpa_commit();
   };
 
-  T acc[4] = {T(0), T(0), T(0), T(0)};
+  T acc[2][4] = {{T(0), T(0), T(0), T(0)}, {T(0), T(0), T(0), T(0)}};
   TileIter<T> ld, cp;
   ld.init(segs, it.seg_begin, it.seg_count);
   cp = ld;
@@ -256,14 +271,19 @@ __global__ void __launch_bounds__(kSkThreads)
     const T *b = Bs + (size_t)st * TN * LDK + n4 * LDK;
 #pragma unroll
     for (int kv = 0; kv < KC / VW; ++kv) {
-      const V av = *reinterpret_cast<const V *>(a + kv * VW);
-      const T *ap = reinterpret_cast<const T *>(&av);
+      const V av0 = *reinterpret_cast<const V *>(a + kv * VW);
+      const V av1 = *reinterpret_cast<const V *>(a + 32 * LDK + kv * VW);
+      const T *ap0 = reinterpret_cast<const T *>(&av0);
+      const T *ap1 = reinterpret_cast<const T *>(&av1);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const V bv = *reinterpret_cast<const V *>(b + j * LDK + kv * VW);
         const T *bp = reinterpret_cast<const T *>(&bv);
 #pragma unroll
-        for (int u = 0; u < VW; ++u) acc[j] += ap[u] * bp[u];
+        for (int u = 0; u < VW; ++u) {
+          acc[0][j] += ap0[u] * bp[u];
+          acc[1][j] += ap1[u] * bp[u];
+        }
       }
     }
     __syncthreads();
@@ -271,13 +291,15 @@ __global__ void __launch_bounds__(kSkThreads)
     cp.next(KC);
   }
   cpa_wait<0>();
-  const int gm = m0 + mm;
-  if (gm < it.M) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int gm = m0 + mm + 32 * h;
+    if (gm >= it.M) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int gn = n0 + n4 + j;
       if (gn >= it.N) break;
-      T v = alpha * acc[j];
+      T v = alpha * acc[h][j];
       if (it.Cin) v += beta * it.Cin[gm + (long long)gn * it.ldcin];
       it.C[gm + (long long)gn * it.ldc] = v;
     }
@@ -296,17 +318,17 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
     HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_tn2_kernel<T>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid(nitems, cdiv(max_m, TM), cdiv(max_n, TN));
-    skinny_tn2_kernel<T><<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);
+    skinny_tn2_kernel<T><<<grid, kTNThreads, smem, s>>>(items, segs, alpha, beta);
   } else {
-    constexpr int KT = sizeof(T) == 4 ? 32 : 16;
-    dim3 grid(nitems, cdiv(max_m, kSkThreads));
+    constexpr int KT = nn_kt<T>();
+    dim3 grid(nitems, cdiv(max_m, kNNRows));
     if (max_n <= 16) {
-      const size_t smem = (size_t)kSkStages * KT * (kSkThreads + 16) * sizeof(T);
+      const size_t smem = (size_t)kSkStages * KT * (kNNRows + 16) * sizeof(T);
       HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_nn2_kernel<T, 16>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       skinny_nn2_kernel<T, 16><<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);
     } else {
-      const size_t smem = (size_t)kSkStages * KT * (kSkThreads + 32) * sizeof(T);
+      const size_t smem = (size_t)kSkStages * KT * (kNNRows + 32) * sizeof(T);
       HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_nn2_kernel<T, 32>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       skinny_nn2_kernel<T, 32><<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);

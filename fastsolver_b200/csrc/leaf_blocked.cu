@@ -535,22 +535,31 @@ __global__ void leaf_init_kernel(const LeafFactorTask<T> *__restrict__ tasks, in
 constexpr int kApplyThreads = 512;
 
 
-// y (kb x MC in shared memory, row stride XS) <- Ainv (kb x kb, column-major, ld nb) y.
-// Ainv is first copied to shared memory `As` (kb x kb, ld kb + 1) with every
-// load independent, so the product runs from shared memory.
+// Stage the diagonal-block inverse Ainv (kb x kb, column-major, ld nb) into
+// shared memory `As` (ld kb + 1) with asynchronous copies (one commit group).
+template <typename T>
+__device__ inline void stage_inverse(const T *__restrict__ Ainv, int nb, int kb, T *As) {
+  const int lds = kb + 1;
+  for (int e = threadIdx.x; e < kb * kb; e += kApplyThreads) {
+    const int i = e % kb, k = e / kb;
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(As + i + k * lds));
+    if (sizeof(T) == 8)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(Ainv + i + (size_t)k * nb));
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(Ainv + i + (size_t)k * nb));
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+// y (kb x MC in shared memory, row stride XS) <- As y, As the staged inverse.
 template <typename T, int MC, int XS>
-__device__ inline void apply_diag(const T *__restrict__ Ainv, int nb, T *y, int kb, T *As) {
+__device__ inline void apply_diag(T *y, int kb, const T *As) {
   constexpr int VW = 16 / sizeof(T);
   constexpr int NV = MC / VW;
   constexpr int OUT = (64 * NV + kApplyThreads - 1) / kApplyThreads;
   using V = typename Vec16<T>::V;
   const int tid = threadIdx.x;
   const int lds = kb + 1;
-  for (int e = tid; e < kb * kb; e += kApplyThreads) {
-    const int i = e % kb, k = e / kb;
-    As[i + k * lds] = Ainv[i + (size_t)k * nb];
-  }
-  __syncthreads();
   T acc[OUT][VW];
 #pragma unroll
   for (int o = 0; o < OUT; ++o) {
@@ -601,13 +610,14 @@ __device__ inline void apply_block(const T *__restrict__ A, long long lda, T *ds
       for (int v = 0; v < VW; ++v) acc[j + v] = xp[v];
     }
     const T *Ai = A + i;
+    constexpr int LB = sizeof(T) == 4 ? 64 : 32;  // loads in flight per row
     int k = 0;
-    for (; k + 16 <= kb; k += 16) {
-      T a[16];
+    for (; k + LB <= kb; k += LB) {
+      T a[LB];
 #pragma unroll
-      for (int u = 0; u < 16; ++u) a[u] = Ai[(long long)(k + u) * lda];
+      for (int u = 0; u < LB; ++u) a[u] = Ai[(long long)(k + u) * lda];
 #pragma unroll
-      for (int u = 0; u < 16; ++u) {
+      for (int u = 0; u < LB; ++u) {
         const T *yk = y + (k + u) * XS;
 #pragma unroll
         for (int j = 0; j < MC; j += VW) {
@@ -647,26 +657,47 @@ __global__ void __launch_bounds__(kApplyThreads)
   const int mc = min(MC, tk.ncols - c0);
   const int tid = threadIdx.x;
   T *xs = reinterpret_cast<T *>(smem_raw);
-  T *As = xs + (size_t)max_n * XS;  // diagonal inverse, nb x (nb + 1)
+  T *As0 = xs + (size_t)max_n * XS;  // two staged inverses, nb x (nb + 1) each
+  const int as_stride = nb * (nb + 1);
   T *X = tk.X + (long long)c0 * tk.ldx;
   const long long ldx = tk.ldx, ldd = tk.ldd;
+  const int np = (n + nb - 1) / nb;
+  // step s < np: forward panel s with Linv_s; step s >= np: backward panel
+  // 2 np - 1 - s with its Uinv.  The next step's inverse is staged while the
+  // current one is applied.
+  auto inv_of = [&](int st, int &k0, int &kb) -> const T * {
+    const int p = st < np ? st : 2 * np - 1 - st;
+    k0 = p * nb;
+    kb = min(nb, n - k0);
+    return (st < np ? tk.Linv : tk.Uinv) + (size_t)p * nb * nb;
+  };
+  {
+    int k0, kb;
+    const T *inv0 = inv_of(0, k0, kb);
+    stage_inverse<T>(inv0, nb, kb, As0);
+  }
   for (int e = tid; e < n * MC; e += kApplyThreads) {
     const int i = e % n, j = e / n;
     xs[i * XS + j] = j < mc ? X[tk.perm[i] + (long long)j * ldx] : T(0);
   }
-  __syncthreads();
-  const int np = (n + nb - 1) / nb;
-  for (int p = 0; p < np; ++p) {
-    const int k0 = p * nb, kb = min(nb, n - k0);
-    apply_diag<T, MC, XS>(tk.Linv + (size_t)p * nb * nb, nb, xs + k0 * XS, kb, As);
-    apply_block<T, MC, XS>(tk.D + (k0 + kb) + (long long)k0 * ldd, ldd, xs + (k0 + kb) * XS,
-                           n - k0 - kb, xs + k0 * XS, kb);
-    __syncthreads();
-  }
-  for (int p = np - 1; p >= 0; --p) {
-    const int k0 = p * nb, kb = min(nb, n - k0);
-    apply_diag<T, MC, XS>(tk.Uinv + (size_t)p * nb * nb, nb, xs + k0 * XS, kb, As);
-    apply_block<T, MC, XS>(tk.D + (long long)k0 * ldd, ldd, xs, k0, xs + k0 * XS, kb);
+  for (int st = 0; st < 2 * np; ++st) {
+    int k0, kb;
+    inv_of(st, k0, kb);
+    if (st + 1 < 2 * np) {
+      int k1, kb1;
+      const T *inv1 = inv_of(st + 1, k1, kb1);
+      stage_inverse<T>(inv1, nb, kb1, As0 + ((st + 1) & 1) * as_stride);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();  // this step's inverse and the previous step's updates visible
+    apply_diag<T, MC, XS>(xs + k0 * XS, kb, As0 + (st & 1) * as_stride);
+    if (st < np)
+      apply_block<T, MC, XS>(tk.D + (k0 + kb) + (long long)k0 * ldd, ldd, xs + (k0 + kb) * XS,
+                             n - k0 - kb, xs + k0 * XS, kb);
+    else
+      apply_block<T, MC, XS>(tk.D + (long long)k0 * ldd, ldd, xs, k0, xs + k0 * XS, kb);
     __syncthreads();
   }
   for (int e = tid; e < n * mc; e += kApplyThreads) {
@@ -749,7 +780,7 @@ template <typename T, int MC>
 void launch_leaf_apply_mc(const LeafFactorTask<T> *tasks, int count, int max_n, int max_cols,
                           int nb, cudaStream_t s) {
   constexpr int XS = MC + 16 / sizeof(T);
-  const size_t smem = ((size_t)max_n * XS + (size_t)nb * (nb + 1)) * sizeof(T);
+  const size_t smem = ((size_t)max_n * XS + 2 * (size_t)nb * (nb + 1)) * sizeof(T);
   HODLR_CUDA_TRY(cudaFuncSetAttribute(leaf_apply_kernel<T, MC>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(cdiv(max_cols, MC), count);
@@ -763,7 +794,7 @@ void launch_leaf_apply(const LeafFactorTask<T> *tasks, int count, int max_n, int
   if (count <= 0 || max_cols <= 0 || max_n <= 0) return;
   if (nb > 64) throw CudaError{cudaErrorInvalidValue};
   // the chunk of P X is max_n x (MC + pad) in shared memory (<= 160 KB)
-  const bool wide_ok = ((size_t)max_n * (32 + 16 / sizeof(T)) + (size_t)nb * (nb + 1)) *
+  const bool wide_ok = ((size_t)max_n * (32 + 16 / sizeof(T)) + 2 * (size_t)nb * (nb + 1)) *
                            sizeof(T) <= 180 * 1024;
   if (max_cols <= 8) launch_leaf_apply_mc<T, 8>(tasks, count, max_n, max_cols, nb, s);
   else if (max_cols <= 16 || !wide_ok) launch_leaf_apply_mc<T, 16>(tasks, count, max_n, max_cols, nb, s);
