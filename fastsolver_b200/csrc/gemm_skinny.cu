@@ -84,17 +84,23 @@ constexpr int kNNRows = 2 * kSkThreads;
 template <typename T>
 __host__ __device__ constexpr int nn_kt() { return sizeof(T) == 4 ? 16 : 8; }
 
+// ring depth: FP64 runs one CTA per SM (register bound) and keeps five tiles
+// in flight; FP32 two CTAs per SM with two each
+template <typename T>
+__host__ __device__ constexpr int nn_stages() { return sizeof(T) == 4 ? 3 : 6; }
+
 template <typename T, int NC>
 __global__ void __launch_bounds__(kSkThreads)
     skinny_nn2_kernel(const GemmItem<T, T> *__restrict__ items, const GemmSeg<T> *__restrict__ segs,
                       T alpha, T beta) {
   constexpr int KT = nn_kt<T>();
+  constexpr int STG = nn_stages<T>();
   constexpr int ROWS = kNNRows;
   constexpr int VW = Vec<T>::W;
   using V = typename Vec<T>::V;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *As = reinterpret_cast<T *>(smem_raw);             // [stage][KT][ROWS]
-  T *Bs = As + (size_t)kSkStages * KT * ROWS;          // [stage][KT][NC]
+  T *Bs = As + (size_t)STG * KT * ROWS;          // [stage][KT][NC]
   const GemmItem<T, T> it = items[blockIdx.x];
   const int row0 = blockIdx.y * ROWS;
   if (row0 >= it.M) return;
@@ -147,16 +153,16 @@ __global__ void __launch_bounds__(kSkThreads)
   ld.init(segs, it.seg_begin, it.seg_count);
   cp = ld;
 #pragma unroll
-  for (int i = 0; i < kSkStages - 1; ++i) {
+  for (int i = 0; i < STG - 1; ++i) {
     load(ld, i);
     if (ld.valid) ld.next(KT);
   }
-  int st = 0, lst = kSkStages - 1;
+  int st = 0, lst = STG - 1;
   while (cp.valid) {
     load(ld, lst);
     if (ld.valid) ld.next(KT);
-    lst = (lst + 1) % kSkStages;
-    cpa_wait<kSkStages - 1>();
+    lst = (lst + 1) % STG;
+    cpa_wait<STG - 1>();
     __syncthreads();
     const T *a = As + (size_t)st * KT * ROWS + tid;
     const T *b = Bs + (size_t)st * KT * NC;
@@ -174,8 +180,8 @@ __global__ void __launch_bounds__(kSkThreads)
         }
       }
     }
-    __syncthreads();  // stage st is refilled kSkStages - 1 tiles later
-    st = (st + 1) % kSkStages;
+    __syncthreads();  // stage st is refilled STG - 1 tiles later
+    st = (st + 1) % STG;
     cp.next(KT);
   }
   cpa_wait<0>();
@@ -323,12 +329,12 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
     constexpr int KT = nn_kt<T>();
     dim3 grid(nitems, cdiv(max_m, kNNRows));
     if (max_n <= 16) {
-      const size_t smem = (size_t)kSkStages * KT * (kNNRows + 16) * sizeof(T);
+      const size_t smem = (size_t)nn_stages<T>() * KT * (kNNRows + 16) * sizeof(T);
       HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_nn2_kernel<T, 16>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       skinny_nn2_kernel<T, 16><<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);
     } else {
-      const size_t smem = (size_t)kSkStages * KT * (kNNRows + 32) * sizeof(T);
+      const size_t smem = (size_t)nn_stages<T>() * KT * (kNNRows + 32) * sizeof(T);
       HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_nn2_kernel<T, 32>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       skinny_nn2_kernel<T, 32><<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);

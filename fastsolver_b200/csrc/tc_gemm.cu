@@ -185,20 +185,25 @@ __device__ inline void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Persistent, warp-specialized split-BF16 GEMM.
+// Persistent, warp-specialized split-operand GEMM.
 //   warps 0-3 (producers): thread p owns row p of the A tile and of the B
 //     tile.  It stages its rows' FP32 values with asynchronous cp.async
-//     copies kStg stages ahead into its own 128-byte slot of a staging ring
-//     (so a per-thread cp.async.wait_group suffices), then splits the landed
-//     stage into bf16 hi / lo and writes the UMMA K-major ring (full[s]:
-//     128 arrivals, empty[s]: tcgen05.commit).
-//   warp 4 lane 0 (MMA issuer): 3 MMAs per 16-deep k-step into one of two TMEM
-//     accumulators (tfull[a]: commit; tready[a]: 128 epilogue arrivals once
-//     the buffer is drained and preloaded with the next tile's scaled Cin).
-//   warps 5-8 (epilogue): thread r owns row r of the tile; it prefetches the
-//     next tile's C row with cp.async as soon as the current tile is drained,
-//     then drains TMEM 16 columns at a time: D = alpha * acc + beta * Cin.
-constexpr int kWarps = 9;
+//     copies kStg stages ahead into its own slot of a staging ring (so a
+//     per-thread cp.async.wait_group suffices), then splits the landed stage
+//     into hi / lo and writes the UMMA K-major ring (full[s]: 128 arrivals,
+//     empty[s]: tcgen05.commit).
+//   warp 4 lane 0 (MMA issuer): 3 MMAs per k-step into one of two TMEM
+//     accumulators (tfull[a]: commit; tready[a]: one arrival per epilogue
+//     thread once the buffer is drained and preloaded with the next tile's
+//     scaled Cin).
+//   warps 5-12 (epilogue): two warps per TMEM lane quarter, each owning one
+//     row of the tile and half of its columns.  Tile j's C is staged by
+//     cp.async while tile j - 1 computes, copied into the accumulator of
+//     tile j before its MMAs (scaled by beta / alpha), and the drain writes
+//     alpha * acc: C = alpha (A B + (beta / alpha) Cin).
+constexpr int kEpiWarps = 8;  // two per TMEM lane quarter, each half of the columns
+constexpr int kEpiThreads = kEpiWarps * 32;
+constexpr int kWarps = 5 + kEpiWarps;
 constexpr int kThreadsP = kWarps * 32;
 constexpr int kStagesP = kTF32 ? 3 : 2;  // UMMA operand ring
 constexpr int kStg = kTF32 ? 4 : 3;      // FP32 staging ring (stages in flight per producer)
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&tfull[a], 1);
-      mbar_init(&tready[a], 128);
+      mbar_init(&tready[a], kEpiThreads);
     }
     mbar_init(&fin, 1);
     abort_sh = 0;
@@ -469,7 +474,9 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     // ------------------------------------------------------------ epilogue
     const int q = warp & 3;        // TMEM lane quarter of this warp
     const int rl = q * 32 + lane;  // row of the tile owned by this thread
-    const int ew = warp - 5;       // epilogue warp 0..3
+    const int ew = warp - 5;       // epilogue warp 0..7
+    const int half = ew >> 2;      // columns [half * BN / 2, (half + 1) * BN / 2)
+    const int cbeg = half * (BN / 2), cend = cbeg + BN / 2;
     int acc = 0;
     uint32_t aphase = 0;
     // Cin staging.  Non-swapped tiles: cst[j * 128 + row] (column j of the
@@ -485,7 +492,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
         if (!SWAP) {
           // lane covers rows m0 + 4 lane .. + 3 of column n0 + j
           const int r4 = m0 + 4 * lane;
-          for (int j = ew; j < BN; j += 4) {
+          for (int j = ew; j < BN; j += kEpiWarps) {
             const int dcol = n0 + j;
             float *dst = cst + j * 128 + 4 * lane;
             const float *src = cin + r4 + (long long)dcol * ld;
@@ -505,7 +512,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
           float *dst = cst + rl * CSTR;
           const float *src = cin + n0 + (long long)gn * ld;
           const bool rowok = gn < Mu;
-          for (int j = 0; j < BN; j += 4) {
+          for (int j = cbeg; j < cend; j += 4) {
             if (vec && rowok && n0 + j + 4 <= Nu) {
               cpa16(dst + j, src + j);
             } else {
@@ -520,17 +527,17 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       }
       cpa_commit();
     };
-    auto epi_sync = [&]() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); };
-    // barrier of the 128 epilogue threads returning the OR of `p` (uniform exit decisions)
+    auto epi_sync = [&]() { asm volatile("bar.sync 1, %0;\n" ::"n"(kEpiThreads) : "memory"); };
+    // barrier of the epilogue threads returning the OR of `p` (uniform exit decisions)
     auto epi_vote_or = [&](bool p) -> bool {
       uint32_t r;
       asm volatile(
           "{\n\t.reg .pred pi, po;\n\t"
           "setp.ne.u32 pi, %1, 0;\n\t"
-          "bar.red.or.pred po, 1, 128, pi;\n\t"
+          "bar.red.or.pred po, 1, %2, pi;\n\t"
           "selp.u32 %0, 1, 0, po;\n\t}\n"
           : "=r"(r)
-          : "r"((uint32_t)p)
+          : "r"((uint32_t)p), "n"(kEpiThreads)
           : "memory");
       return r != 0;
     };
@@ -560,7 +567,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     auto preload = [&](const Tile &T, int b) {
       if (!(T.it.Cin != nullptr && beta != 0.f)) return;
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 16) {
+      for (int c0 = cbeg; c0 < cend; c0 += 16) {
         uint32_t r[16];
         if (!SWAP) {
           const float *cs = cst + c0 * 128 + rl;
@@ -630,7 +637,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       const long long ldc = it.ldc;
       const float a_eff = live ? alpha : 0.f;
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN && n0 + c0 < Nu; c0 += 16) {
+      for (int c0 = cbeg; c0 < cend && n0 + c0 < Nu; c0 += 16) {
         uint32_t r[16];
         const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + c0);
         asm volatile(
