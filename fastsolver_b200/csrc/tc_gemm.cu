@@ -186,24 +186,27 @@ __device__ inline void mbar_arrive(uint64_t *bar) {
 }
 
 // Persistent, warp-specialized split-operand GEMM.
-//   warps 0-3 (producers): thread p owns row p of the A tile and of the B
-//     tile.  It stages its rows' FP32 values with asynchronous cp.async
+//   warps 0-7 (producers): thread p of warps 0-3 owns row p of the A tile,
+//     of warps 4-7 row p of the B tile.  It stages its rows' FP32 values with asynchronous cp.async
 //     copies kStg stages ahead into its own slot of a staging ring (so a
 //     per-thread cp.async.wait_group suffices), then splits the landed stage
 //     into hi / lo and writes the UMMA K-major ring (full[s]: 128 arrivals,
 //     empty[s]: tcgen05.commit).
-//   warp 4 lane 0 (MMA issuer): 3 MMAs per k-step into one of two TMEM
+//   warp 8 lane 0 (MMA issuer): 3 MMAs per k-step into one of two TMEM
 //     accumulators (tfull[a]: commit; tready[a]: one arrival per epilogue
 //     thread once the buffer is drained and preloaded with the next tile's
 //     scaled Cin).
-//   warps 5-12 (epilogue): two warps per TMEM lane quarter, each owning one
+//   warps 9-16 (epilogue): two warps per TMEM lane quarter, each owning one
 //     row of the tile and half of its columns.  Tile j's C is staged by
 //     cp.async while tile j - 1 computes, copied into the accumulator of
 //     tile j before its MMAs (scaled by beta / alpha), and the drain writes
 //     alpha * acc: C = alpha (A B + (beta / alpha) Cin).
 constexpr int kEpiWarps = 8;  // two per TMEM lane quarter, each half of the columns
 constexpr int kEpiThreads = kEpiWarps * 32;
-constexpr int kWarps = 5 + kEpiWarps;
+constexpr int kProdWarps = 8;  // 4 for the A tile rows, 4 for the B tile rows
+constexpr int kMmaWarp = kProdWarps;
+constexpr int kEpiWarp0 = kProdWarps + 1;
+constexpr int kWarps = kProdWarps + 1 + kEpiWarps;
 constexpr int kThreadsP = kWarps * 32;
 constexpr int kStagesP = kTF32 ? 3 : 2;  // UMMA operand ring
 constexpr int kStg = kTF32 ? 4 : 3;      // FP32 staging ring (stages in flight per producer)
@@ -296,7 +299,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
 
   if (tid == 0) {
     for (int s = 0; s < kStagesP; ++s) {
-      mbar_init(&full[s], 128);
+      mbar_init(&full[s], kProdWarps * 32);
       mbar_init(&empty[s], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -366,26 +369,27 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     first_in_tile(ps);
   };
 
-  if (warp < 4) {
+  if (warp < kProdWarps) {
     // ------------------------------------------------------------ producers
-    const int p = tid;
+    // warps 0-3 stage and split row p of the A tile, warps 4-7 row p of the
+    // B tile (rows p >= BN of B do not exist)
+    const bool isB = warp >= 4;
+    const int p = tid & 127;
+    const int sw = kTF32 ? ((p >> 1) & 3) : (p & 7);
     KPos<TC> iss, con;
     iss.t = con.t = blockIdx.x;
     first_in_tile(iss);
     first_in_tile(con);
     auto issue = [&](KPos<TC> &ps, int slot) {
-      float *a = stg + slot * (STG_BYTES / 4) + p * BK;
-      float *b = a + 128 * BK;
+      float *row = stg + slot * (STG_BYTES / 4) + (isB ? 128 * BK : 0) + p * BK;
       if (ps.valid) {
         const GemmSeg<float> &sg = ps.sg;
-        const int sw = kTF32 ? ((p >> 1) & 3) : (p & 7);
-        if (!swap) {
-          stage_row(a, sw, sg.A, sg.lda, trans != 0, ps.m0 + p, ps.it.M, ps.k0, sg.K);
-          stage_row(b, sw, sg.B, sg.ldb, true, ps.n0 + p, p < BN ? ps.it.N : -1, ps.k0, sg.K);
-        } else {
-          stage_row(a, sw, sg.B, sg.ldb, true, ps.m0 + p, ps.it.N, ps.k0, sg.K);
-          stage_row(b, sw, sg.A, sg.lda, trans != 0, ps.n0 + p, p < BN ? ps.it.M : -1, ps.k0,
-                    sg.K);
+        if (!isB) {
+          if (!swap) stage_row(row, sw, sg.A, sg.lda, trans != 0, ps.m0 + p, ps.it.M, ps.k0, sg.K);
+          else stage_row(row, sw, sg.B, sg.ldb, true, ps.m0 + p, ps.it.N, ps.k0, sg.K);
+        } else if (p < BN) {
+          if (!swap) stage_row(row, sw, sg.B, sg.ldb, true, ps.n0 + p, ps.it.N, ps.k0, sg.K);
+          else stage_row(row, sw, sg.A, sg.lda, trans != 0, ps.n0 + p, ps.it.M, ps.k0, sg.K);
         }
         next(ps);
       }
@@ -399,29 +403,24 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       issue(iss, islot);
       islot = (islot + 1) % kStg;
       cpa_wait<kStg - 1>();  // this thread's copies of stage `cslot` have landed
-      const float *a = stg + cslot * (STG_BYTES / 4) + p * BK;
-      const float *b = a + 128 * BK;
-      float va[BK], vb[BK];
+      const float *row = stg + cslot * (STG_BYTES / 4) + (isB ? 128 * BK : 0) + p * BK;
+      float v[BK];
 #pragma unroll
       for (int q = 0; q < BK / 4; ++q) {
-        const int qs = q ^ (kTF32 ? ((p >> 1) & 3) : (p & 7));
-        const float4 x = reinterpret_cast<const float4 *>(a)[qs];
-        const float4 y = reinterpret_cast<const float4 *>(b)[qs];
-        va[4 * q] = x.x; va[4 * q + 1] = x.y; va[4 * q + 2] = x.z; va[4 * q + 3] = x.w;
-        vb[4 * q] = y.x; vb[4 * q + 1] = y.y; vb[4 * q + 2] = y.z; vb[4 * q + 3] = y.w;
+        const float4 x = reinterpret_cast<const float4 *>(row)[q ^ sw];
+        v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
       }
       cslot = (cslot + 1) % kStg;
       if (!mbar_wait(&empty[stage], phase ^ 1)) { abort_sh = 1; break; }
       unsigned char *base = ring + stage * STAGE_BYTES;
-      unsigned char *ahi = base, *alo = base + A_BYTES;
-      unsigned char *bhi = base + 2 * A_BYTES, *blo = bhi + B_BYTES;
+      if (!isB) {
+        unsigned char *ahi = base, *alo = base + A_BYTES;
 #pragma unroll
-      for (int c = 0; c < 4; ++c)
-        split_chunk(va + (16 / ELEM) * c, ahi, alo, kmajor_off(BM, p, c));
-      if (p < BN) {
+        for (int c = 0; c < 4; ++c) split_chunk(v + (16 / ELEM) * c, ahi, alo, kmajor_off(BM, p, c));
+      } else if (p < BN) {
+        unsigned char *bhi = base + 2 * A_BYTES, *blo = bhi + B_BYTES;
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
-          split_chunk(vb + (16 / ELEM) * c, bhi, blo, kmajor_off(BN, p, c));
+        for (int c = 0; c < 4; ++c) split_chunk(v + (16 / ELEM) * c, bhi, blo, kmajor_off(BN, p, c));
       }
       fence_proxy_async();
       mbar_arrive(&full[stage]);
@@ -429,7 +428,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       next(con);
     }
     cpa_wait<0>();
-  } else if (warp == 4) {
+  } else if (warp == kMmaWarp) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
       const uint32_t idesc = instr_desc(BM, BN);
@@ -474,7 +473,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     // ------------------------------------------------------------ epilogue
     const int q = warp & 3;        // TMEM lane quarter of this warp
     const int rl = q * 32 + lane;  // row of the tile owned by this thread
-    const int ew = warp - 5;       // epilogue warp 0..7
+    const int ew = warp - kEpiWarp0;  // epilogue warp 0..7
     const int half = ew >> 2;      // columns [half * BN / 2, (half + 1) * BN / 2)
     const int cbeg = half * (BN / 2), cend = cbeg + BN / 2;
     int acc = 0;
