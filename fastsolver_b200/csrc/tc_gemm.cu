@@ -275,6 +275,32 @@ __device__ inline void stage_row(float *dst, int sw, const float *base, long lon
   }
 }
 
+// Stage a K x rows column-major operand block (rows contiguous in memory) as
+// a [BK][128] column tile, cooperatively: warp w of the 4-warp group copies
+// k-columns w, w + 4, ...; lane l copies rows 4 l .. 4 l + 3 with one 16-byte
+// copy when the block is aligned and fully inside the matrix.
+__device__ inline void stage_cols(float *dst, int wg, int lane, const float *base, long long ld,
+                                  int row0, int rows_valid, int k0, int K) {
+  const int r = row0 + 4 * lane;
+  const bool vec = ((reinterpret_cast<uintptr_t>(base) & 15) == 0) && ((ld & 3) == 0);
+#pragma unroll
+  for (int kk = 0; kk < BK / 4; ++kk) {
+    const int k = wg + 4 * kk;
+    float *d = dst + k * 128 + 4 * lane;
+    const float *src = base + r + (long long)(k0 + k) * ld;
+    const bool kin = k0 + k < K;
+    if (vec && kin && r + 4 <= rows_valid) {
+      cpa16(d, src);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool ok = kin && r + u < rows_valid;
+        cpa4(d + u, ok ? src + u : base, ok);
+      }
+    }
+  }
+}
+
 template <int BN, bool SWAP, typename TC>
 __global__ void __launch_bounds__(kThreadsP, 1)
     tc_gemm_persistent(const GemmItem<float, TC> *__restrict__ items,
@@ -380,16 +406,31 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     iss.t = con.t = blockIdx.x;
     first_in_tile(iss);
     first_in_tile(con);
+    // the non-K-contiguous operand (A when !trans) is staged column-wise by
+    // its whole 4-warp group; the other one row-wise by each thread
+    // (measured: worth it for the non-swapped A tile only; the swapped items'
+    // non-contiguous operand has BN <= 64 rows and stays row-wise)
+    const bool colmode = !isB && !swap && trans == 0;
+    const int gbar = isB ? 3 : 2;  // named barrier of this producer group
+    auto group_sync = [&]() { asm volatile("bar.sync %0, 128;\n" ::"r"(gbar) : "memory"); };
     auto issue = [&](KPos<TC> &ps, int slot) {
-      float *row = stg + slot * (STG_BYTES / 4) + (isB ? 128 * BK : 0) + p * BK;
+      float *region = stg + slot * (STG_BYTES / 4) + (isB ? 128 * BK : 0);
+      float *row = region + p * BK;
       if (ps.valid) {
         const GemmSeg<float> &sg = ps.sg;
         if (!isB) {
-          if (!swap) stage_row(row, sw, sg.A, sg.lda, trans != 0, ps.m0 + p, ps.it.M, ps.k0, sg.K);
-          else stage_row(row, sw, sg.B, sg.ldb, true, ps.m0 + p, ps.it.N, ps.k0, sg.K);
-        } else if (p < BN) {
-          if (!swap) stage_row(row, sw, sg.B, sg.ldb, true, ps.n0 + p, ps.it.N, ps.k0, sg.K);
-          else stage_row(row, sw, sg.A, sg.lda, trans != 0, ps.n0 + p, ps.it.M, ps.k0, sg.K);
+          if (!swap) {
+            if (colmode) stage_cols(region, warp & 3, lane, sg.A, sg.lda, ps.m0, ps.it.M, ps.k0, sg.K);
+            else stage_row(row, sw, sg.A, sg.lda, trans != 0, ps.m0 + p, ps.it.M, ps.k0, sg.K);
+          } else {
+            stage_row(row, sw, sg.B, sg.ldb, true, ps.m0 + p, ps.it.N, ps.k0, sg.K);
+          }
+        } else {
+          if (!swap) {
+            if (p < BN) stage_row(row, sw, sg.B, sg.ldb, true, ps.n0 + p, ps.it.N, ps.k0, sg.K);
+          } else if (p < BN) {
+            stage_row(row, sw, sg.A, sg.lda, trans != 0, ps.n0 + p, ps.it.M, ps.k0, sg.K);
+          }
         }
         next(ps);
       }
@@ -399,19 +440,50 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     for (int i = 0; i < kStg - 1; ++i) { issue(iss, islot); islot = (islot + 1) % kStg; }
     int stage = 0, cslot = 0;
     uint32_t phase = 0;
-    while (con.valid && !abort_sh) {
+    // exit decision: uniform within a group that shares barriers (a thread
+    // whose wait timed out raises abort_sh and the next vote ends the group)
+    auto group_vote_or = [&](bool pr) -> bool {
+      uint32_t r;
+      asm volatile(
+          "{\n\t.reg .pred pi, po;\n\t"
+          "setp.ne.u32 pi, %1, 0;\n\t"
+          "bar.red.or.pred po, %2, 128, pi;\n\t"
+          "selp.u32 %0, 1, 0, po;\n\t}\n"
+          : "=r"(r)
+          : "r"((uint32_t)pr), "r"(gbar)
+          : "memory");
+      return r != 0;
+    };
+    while (true) {
+      if (colmode) {
+        if (group_vote_or(!con.valid || abort_sh)) break;
+      } else if (!con.valid || abort_sh) {
+        break;
+      }
       issue(iss, islot);
       islot = (islot + 1) % kStg;
       cpa_wait<kStg - 1>();  // this thread's copies of stage `cslot` have landed
-      const float *row = stg + cslot * (STG_BYTES / 4) + (isB ? 128 * BK : 0) + p * BK;
+      const float *region = stg + cslot * (STG_BYTES / 4) + (isB ? 128 * BK : 0);
       float v[BK];
+      if (colmode) {
+        group_sync();  // the group's copies of this stage have landed
 #pragma unroll
-      for (int q = 0; q < BK / 4; ++q) {
-        const float4 x = reinterpret_cast<const float4 *>(row)[q ^ sw];
-        v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+        for (int k = 0; k < BK; ++k) v[k] = region[k * 128 + p];
+        group_sync();  // every thread has read the slot before it is refilled
+      } else {
+        const float *row = region + p * BK;
+#pragma unroll
+        for (int q = 0; q < BK / 4; ++q) {
+          const float4 x = reinterpret_cast<const float4 *>(row)[q ^ sw];
+          v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+        }
       }
       cslot = (cslot + 1) % kStg;
-      if (!mbar_wait(&empty[stage], phase ^ 1)) { abort_sh = 1; break; }
+      if (!mbar_wait(&empty[stage], phase ^ 1)) {
+        abort_sh = 1;
+        if (!colmode) break;
+        continue;  // the group leaves together at the next vote
+      }
       unsigned char *base = ring + stage * STAGE_BYTES;
       if (!isB) {
         unsigned char *ahi = base, *alo = base + A_BYTES;
