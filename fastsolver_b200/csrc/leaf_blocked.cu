@@ -303,84 +303,110 @@ __global__ void __launch_bounds__(kRegThreads, 1)
   bool warp_live = __any_sync(0xffffffffu, live[0]);
   int info_local = 0;
   bool swaps = false;
+  // The columns are factored QW at a time by one unrolled body inside a
+  // runtime loop (a quarter of the code of a fully unrolled panel, which
+  // kept missing the instruction cache): before quarter h every row is
+  // rotated left by h QW, so the quarter's columns sit at register positions
+  // 0 .. QW - 1; positions QW .. NB - h QW - 1 hold the later quarters (they
+  // are updated), the rest the finished ones (left alone).
+  constexpr int QW = NB < 16 ? NB : 16;
+  constexpr int NQ = NB / QW;
+#pragma unroll 1
+  for (int h = 0; h < NQ; ++h) {
+    const int live_blocks = NQ - h;  // blocks of QW positions still being updated
 #pragma unroll
-  for (int j = 0; j < NB; ++j) {
-    if (j >= kb) break;
-    const int slot = j & 1;
-    if (warp_live) {
-      T best = T(0);
-      int bp = 0x7fffffff, bc = -1;
+    for (int jj = 0; jj < QW; ++jj) {
+      const int j = h * QW + jj;  // panel column
+      if (j < kb) {
+        const int slot = j & 1;
+        if (warp_live) {
+          T best = T(0);
+          int bp = 0x7fffffff, bc = -1;
 #pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        if (live[q] && pos[q] >= j) {
-          const T av = tabs(a[q][j]);
-          // NaN is never a candidate (as idamax, which skips it)
-          if (av == av && (bp == 0x7fffffff || av > best || (av == best && pos[q] < bp))) {
-            best = av; bp = pos[q]; bc = tid + q * kRegThreads;
+          for (int q = 0; q < RPT; ++q) {
+            if (live[q] && pos[q] >= j) {
+              const T av = tabs(a[q][jj]);
+              // NaN is never a candidate (as idamax, which skips it)
+              if (av == av && (bp == 0x7fffffff || av > best || (av == best && pos[q] < bp))) {
+                best = av; bp = pos[q]; bc = tid + q * kRegThreads;
+              }
+            }
           }
-        }
-      }
-      int wl;
-      warp_argmax(best, bp, bc, wl);
-      // the winning lane publishes its row
+          int wl;
+          warp_argmax(best, bp, bc, wl);
+          // the winning lane publishes its row (rotated like every row)
 #pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        if (bc >= 0 && bc == tid + q * kRegThreads) {
-          V *dst = reinterpret_cast<V *>(wrow[slot][warp]);
+          for (int q = 0; q < RPT; ++q) {
+            if (bc >= 0 && bc == tid + q * kRegThreads) {
+              V *dst = reinterpret_cast<V *>(wrow[slot][warp]);
 #pragma unroll
-          for (int cv = 0; cv < NB / VW; ++cv) {
-            V v;
-            T *vp = reinterpret_cast<T *>(&v);
+              for (int cv = 0; cv < NB / VW; ++cv) {
+                V v;
+                T *vp = reinterpret_cast<T *>(&v);
 #pragma unroll
-            for (int u = 0; u < VW; ++u) vp[u] = a[q][cv * VW + u];
-            dst[cv] = v;
+                for (int u = 0; u < VW; ++u) vp[u] = a[q][cv * VW + u];
+                dst[cv] = v;
+              }
+            }
           }
+          if (lane == 0) { wval[slot][warp] = best; wpos[slot][warp] = bp; wcode[slot][warp] = bc; }
+        } else if (lane == 0) {
+          wval[slot][warp] = T(0); wpos[slot][warp] = 0x7fffffff; wcode[slot][warp] = -1;
         }
-      }
-      if (lane == 0) { wval[slot][warp] = best; wpos[slot][warp] = bp; wcode[slot][warp] = bc; }
-    } else if (lane == 0) {
-      wval[slot][warp] = T(0); wpos[slot][warp] = 0x7fffffff; wcode[slot][warp] = -1;
-    }
-    __syncthreads();
-    // combine the warp candidates (every thread, same result)
-    T pb = T(0);
-    int pp = 0x7fffffff, pc = -1, pw = 0;
-    if (lane < NW) { pb = wval[slot][lane]; pp = wpos[slot][lane]; pc = wcode[slot][lane]; }
-    warp_argmax(pb, pp, pc, pw);  // pw: the winning warp
-    int p = j;
-    T piv = T(0);
-    if (pc >= 0) { p = pp; piv = wrow[slot][pw][j]; }
-    if (tid == 0) pv[j] = p;
-    if (p != j) swaps = true;
-    if (warp_live) {
+        __syncthreads();
+        // combine the warp candidates (every thread, same result)
+        T pb = T(0);
+        int pp = 0x7fffffff, pc = -1, pw = 0;
+        if (lane < NW) { pb = wval[slot][lane]; pp = wpos[slot][lane]; pc = wcode[slot][lane]; }
+        warp_argmax(pb, pp, pc, pw);  // pw: the winning warp
+        int p = j;
+        T piv = T(0);
+        if (pc >= 0) { p = pp; piv = wrow[slot][pw][jj]; }
+        if (tid == 0) pv[j] = p;
+        if (p != j) swaps = true;
+        if (warp_live) {
 #pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        if (live[q]) {
-          if (tid + q * kRegThreads == pc) pos[q] = j;
-          else if (pos[q] == j) pos[q] = p;
-        }
-      }
-      if (piv != T(0)) {
-        const T rinv = sizeof(T) == 4 ? T(__frcp_rn(float(piv))) : T(__drcp_rn(double(piv)));
-        const V *prow = reinterpret_cast<const V *>(wrow[slot][pw]);
+          for (int q = 0; q < RPT; ++q) {
+            if (live[q]) {
+              if (tid + q * kRegThreads == pc) pos[q] = j;
+              else if (pos[q] == j) pos[q] = p;
+            }
+          }
+          if (piv != T(0)) {
+            const T rinv = sizeof(T) == 4 ? T(__frcp_rn(float(piv))) : T(__drcp_rn(double(piv)));
+            const V *prow = reinterpret_cast<const V *>(wrow[slot][pw]);
 #pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          if (live[q] && pos[q] > j) {
-            const T l = a[q][j] * rinv;
-            a[q][j] = l;
+            for (int q = 0; q < RPT; ++q) {
+              if (live[q] && pos[q] > j) {
+                const T l = a[q][jj] * rinv;
+                a[q][jj] = l;
 #pragma unroll
-            for (int cv = (j + 1) / VW; cv < NB / VW; ++cv) {
-              const V v = prow[cv];
-              const T *vp = reinterpret_cast<const T *>(&v);
+                for (int cv = (jj + 1) / VW; cv < NB / VW; ++cv) {
+                  if (cv * VW >= QW && (cv * VW) / QW >= live_blocks) continue;
+                  const V v = prow[cv];
+                  const T *vp = reinterpret_cast<const T *>(&v);
 #pragma unroll
-              for (int u = 0; u < VW; ++u)
-                if (cv * VW + u > j) a[q][cv * VW + u] -= l * vp[u];
+                  for (int u = 0; u < VW; ++u)
+                    if (cv * VW + u > jj) a[q][cv * VW + u] -= l * vp[u];
+                }
+              }
             }
           }
         }
+        if (piv == T(0) && info_local == 0) info_local = k0 + j + 1;
       }
     }
-    if (piv == T(0) && info_local == 0) info_local = k0 + j + 1;
+    // rotate every row left by QW (after NQ rotations the order is restored)
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      T t[QW];
+#pragma unroll
+      for (int c = 0; c < QW; ++c) t[c] = a[q][c];
+#pragma unroll
+      for (int c = 0; c < NB - QW; ++c) a[q][c] = a[q][c + QW];
+#pragma unroll
+      for (int c = 0; c < QW; ++c) a[q][NB - QW + c] = t[c];
+    }
   }
   // rows to their final positions; diagonal block rows to shared memory
   int pold[RPT];
