@@ -51,7 +51,12 @@ constexpr bool kTF32 = false;
 constexpr int ELEM = kTF32 ? 4 : 2;  // bytes per split operand element
 constexpr int BK = 64 / ELEM;        // K per stage
 constexpr int MMA_K = 32 / ELEM;     // K per tcgen05.mma
-constexpr long long kSpinLimit = 1LL << 26;
+// Bounded mbarrier waits: each try_wait may suspend the thread for up to
+// kSuspendNs (it returns as soon as the phase completes), so waiting warps
+// do not take issue slots from the working ones; kSpinLimit tries bound the
+// wait to a few seconds before the kernel gives up.
+constexpr long long kSpinLimit = 1LL << 22;
+constexpr unsigned kSuspendNs = 1000;
 
 __device__ inline uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -68,10 +73,10 @@ __device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(ok)
-        : "r"(a), "r"(parity)
+        : "r"(a), "r"(parity), "r"(kSuspendNs)
         : "memory");
     if (ok) return true;
   }
