@@ -32,18 +32,38 @@ namespace hodlr {
 
 namespace {
 
-constexpr int kNodeThreads = 1024;
+constexpr int kNodeThreads = 256;
 constexpr int kNodeWarps = kNodeThreads / 32;
 
 }  // namespace
 
 // doubles of the factor kernel's shared memory before the staged operands:
-// A (s x (s + 1)), rowk, colk (s each), piv, src (s ints each), rounded up
+// A (s x (s + 1)), rowk, colk (s each), piv, src, at (s ints each), rounded up
 __host__ __device__ size_t node_factor_words(int max_s) {
-  return (size_t)max_s * (max_s + 1) + 2 * (size_t)max_s + (size_t)max_s + 2;
+  return (size_t)max_s * (max_s + 1) + 2 * (size_t)max_s + 2 * (size_t)max_s + 2;
 }
 
 namespace {
+
+// Warp-wide argmax of |a| (>= 0, so its bit pattern orders like the value)
+// with the lowest position on ties; lanes without a candidate pass
+// pos = INT_MAX.  Every lane gets the winner's (best, pos, code); pos stays
+// INT_MAX (code -1) when no lane had a candidate.
+__device__ inline void warp_argmax_f64(double &best, int &pos, int &code, int &wlane) {
+  const bool cand = pos != 0x7fffffff;
+  const unsigned long long b = cand ? (unsigned long long)__double_as_longlong(best) : 0ull;
+  const unsigned hi = (unsigned)(b >> 32), lo = (unsigned)b;
+  const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+  const bool top = hi == mh && lo == ml;
+  const unsigned pm = __reduce_min_sync(0xffffffffu, top ? (unsigned)pos : 0xffffffffu);
+  const unsigned win = __ballot_sync(0xffffffffu, cand && top && (unsigned)pos == pm);
+  wlane = win ? __ffs(win) - 1 : 0;
+  best = __longlong_as_double((long long)(((unsigned long long)mh << 32) | ml));
+  pos = win ? (int)pm : 0x7fffffff;
+  code = __shfl_sync(0xffffffffu, code, wlane);
+  if (!win) code = -1;
+}
 
 // out(i, c) = [i == c] (if add_identity) + alpha * sum_k a(i, k) b(k, c) for
 // i < rows, c < cols: lanes over rows, warps over columns, 2 x 2 outputs per
@@ -79,7 +99,7 @@ __device__ inline void node_product(int rows, int cols, int K, double alpha, boo
   }
 }
 
-template <typename TW, typename TE>
+template <typename TW, typename TE, int RL>
 __global__ void __launch_bounds__(kNodeThreads)
     node_factor_kernel(const NodeTask<TW, TE> *tasks, int form, int max_s, int max_r, int stage,
                        int *info) {
@@ -90,14 +110,15 @@ __global__ void __launch_bounds__(kNodeThreads)
   const int s = form == 0 ? r0 : s2;
   const int lda = s + 1;                              // row stride (odd: no bank conflicts)
   double *A = reinterpret_cast<double *>(smem_raw);   // s x s, row-major
-  double *rowk = A + (size_t)s * lda;
-  double *colk = rowk + s;
-  int *piv = reinterpret_cast<int *>(colk + s);
+  // two s-double slots after A are spare; the int arrays follow them
+  int *piv = reinterpret_cast<int *>(A + (size_t)s * lda + 2 * s);
   int *src = piv + s;
+  int *at = src + s;
   // form 0 with stage != 0: V0Tu0, V1Tu1 and G0 as FP64 in shared memory
   double *W0s = reinterpret_cast<double *>(smem_raw) + node_factor_words(max_s);
   double *W1s = W0s + (size_t)max_r * max_r;
   double *Gs = W1s + (size_t)max_r * max_r;
+  double *Ss = Gs + (size_t)max_r * max_r;  // S^{-1} un-permuted, column-major (staged form 0)
   __shared__ int s_info;
 
   if (tid == 0) s_info = 0;
@@ -127,86 +148,131 @@ __global__ void __launch_bounds__(kNodeThreads)
   }
   __syncthreads();
 
-  // ---- Gauss-Jordan: A <- (P S)^{-1} in place, two barriers per column
-  for (int k = 0; k < s; ++k) {
-    if (warp == 0) {
-      double best = -1.0;
-      int bi = s;
-      for (int i = k + lane; i < s; i += 32) {
-        const double a = fabs(A[i * lda + k]);
-        if (a > best) { best = a; bi = i; }
-      }
+  // ---- Gauss-Jordan with implicit row interchanges, one barrier per column.
+  // Rows never move; every warp finds the pivot of column k itself (largest
+  // |a| among the rows not yet pivotal, lowest current position on ties, as
+  // idamax after LAPACK's interchanges) and keeps identical copies of the
+  // rows' current positions.  Warp w eliminates column k from rows w, w + 8,
+  // ... with the (unscaled) pivot row; the pivot row itself is scaled by its
+  // owner at the start of the next step, when nobody else reads it.
+  // RL: rows (and columns) per lane, ceil(max_s / 32)
+  int posr[RL];
+  bool usedr[RL];
 #pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ob = __shfl_down_sync(0xffffffffu, best, off);
-        const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-      }
-      bi = __shfl_sync(0xffffffffu, bi, 0);
-      if (bi >= s) bi = k;  // NaN column: keep the diagonal
-      if (bi != k)
-        for (int c = lane; c < s; c += 32) {
-          const double t = A[k * lda + c];
-          A[k * lda + c] = A[bi * lda + c];
-          A[bi * lda + c] = t;
+  for (int t = 0; t < RL; ++t) {
+    const int row = lane + 32 * t;
+    posr[t] = row;
+    usedr[t] = row >= s;
+  }
+  int prevp = -1, prevk = -1;
+  double prevr = 0.0;
+  auto scale_prev = [&]() {
+    if (prevp >= 0 && (prevp % kNodeWarps) == warp) {
+      double *Ap = A + prevp * lda;
+      for (int c = lane; c < s; c += 32) Ap[c] = (c == prevk) ? prevr : Ap[c] * prevr;
+    }
+  };
+  for (int k = 0; k < s; ++k) {
+    scale_prev();
+    double best = 0.0;
+    int bp = 0x7fffffff, code = -1;
+#pragma unroll
+    for (int t = 0; t < RL; ++t) {
+      const int row = lane + 32 * t;
+      if (row < s && !usedr[t]) {
+        const double av = fabs(A[row * lda + k]);
+        if (av == av && (bp == 0x7fffffff || av > best || (av == best && posr[t] < bp))) {
+          best = av; bp = posr[t]; code = row;
         }
+      }
+    }
+    int wl;
+    warp_argmax_f64(best, bp, code, wl);
+    const int p = code, pp = bp;
+    const double pk = p >= 0 ? A[p * lda + k] : 0.0;
+    if (pk == 0.0) {  // exactly singular (or a NaN column): INFO = k + 1, uniform
+      if (tid == 0) s_info = k + 1;
+      break;
+    }
+#pragma unroll
+    for (int t = 0; t < RL; ++t) {
+      const int row = lane + 32 * t;
+      if (row == p) { posr[t] = k; usedr[t] = true; }
+      else if (posr[t] == k) posr[t] = pp;
+    }
+    if (tid == 0) piv[k] = pp;
+    const double rinv = 1.0 / pk;
+    double prow[RL];
+#pragma unroll
+    for (int u = 0; u < RL; ++u) {
+      const int c = lane + 32 * u;
+      prow[u] = c < s ? A[p * lda + c] : 0.0;
+    }
+    for (int i = warp; i < s; i += kNodeWarps) {
+      if (i == p) continue;
+      double *Ai = A + i * lda;
+      const double f = Ai[k] * rinv;
       __syncwarp();
-      for (int c = lane; c < s; c += 32) rowk[c] = A[k * lda + c];
-      for (int i = lane; i < s; i += 32) colk[i] = A[i * lda + k];
-      if (lane == 0) {
-        piv[k] = bi;
-        if (A[k * lda + k] == 0.0 && s_info == 0) s_info = k + 1;
+#pragma unroll
+      for (int u = 0; u < RL; ++u) {
+        const int c = lane + 32 * u;
+        if (c < s) Ai[c] = (c == k) ? -f : Ai[c] - f * prow[u];
       }
     }
-    __syncthreads();
-    const double pk = rowk[k];
-    if (pk != 0.0) {
-      const double rinv = 1.0 / pk;
-      for (int i = warp; i < s; i += kNodeWarps) {
-        const double f = colk[i] * rinv;
-        double *Ai = A + i * lda;
-        if (i == k) {
-          for (int c = lane; c < s; c += 32) Ai[c] = (c == k ? 1.0 : rowk[c]) * rinv;
-        } else {
-          for (int c = lane; c < s; c += 32)
-            Ai[c] = (c == k ? 0.0 : Ai[c]) - f * (c == k ? 1.0 : rowk[c]);
-        }
-      }
-    }
+    prevp = p;
+    prevk = k;
+    prevr = rinv;
     __syncthreads();
   }
+  __syncthreads();  // s_info (set on the singular break) visible to all
+  if (s_info == 0) scale_prev();
+  // at[i]: the storage row at final position i (every warp holds the same posr)
+  if (warp == 0) {
+#pragma unroll
+    for (int t = 0; t < RL; ++t) {
+      const int row = lane + 32 * t;
+      if (row < s) at[posr[t]] = row;
+    }
+  }
+  __syncthreads();
   if (tid == 0) {
     if (info) info[tk.info_slot] = s_info;
     // undo the row interchanges as column interchanges, last pivot first
     for (int j = 0; j < s; ++j) src[j] = j;
-    for (int k = s - 1; k >= 0; --k) {
-      const int p = piv[k];
-      const int t = src[k];
-      src[k] = src[p];
-      src[p] = t;
-    }
+    if (s_info == 0)
+      for (int k = s - 1; k >= 0; --k) {
+        const int p = piv[k];
+        const int t = src[k];
+        src[k] = src[p];
+        src[p] = t;
+      }
   }
   __syncthreads();
   if (s_info != 0) return;  // singular: no solve matrix (uniform across the CTA)
-  // S^{-1}(i, j) = A[i][src[j]]
+  // S^{-1}(i, j) = A[at[i]][src[j]]
   const long long ldm = s2;
   TE *M = tk.M;
   if (form == 1) {
     for (int e = tid; e < s * s; e += kNodeThreads) {
       const int i = e % s, j = e / s;
-      M[i + (long long)j * ldm] = TE(A[i * lda + src[j]]);
+      M[i + (long long)j * ldm] = TE(A[at[i] * lda + src[j]]);
     }
     return;
   }
   // form 0: the blocks of M around S^{-1} (r0 x r0)
   for (int e = tid; e < r0 * r0; e += kNodeThreads) {
     const int i = e % r0, j = e / r0;
-    M[i + (long long)(r1 + j) * ldm] = TE(A[i * lda + src[j]]);
+    M[i + (long long)(r1 + j) * ldm] = TE(A[at[i] * lda + src[j]]);
   }
   if (stage) {
+    for (int e = tid; e < r0 * r0; e += kNodeThreads) {
+      const int i = e % r0, j = e / r0;
+      Ss[e] = A[at[i] * lda + src[j]];
+    }
+    __syncthreads();
     // G0 = -S^{-1} V1Tu1 (r0 x r1): M's upper left block, kept for the last product
     node_product(
-        r0, r1, r0, -1.0, false, [&](int i, int k) { return A[i * lda + src[k]]; },
+        r0, r1, r0, -1.0, false, [&](int i, int k) { return Ss[i + k * r0]; },
         [&](int k, int c) { return W1s[k + c * r0]; },
         [&](int i, int c, double v) {
           Gs[i + c * r0] = v;
@@ -215,7 +281,7 @@ __global__ void __launch_bounds__(kNodeThreads)
     // -V0Tu0 S^{-1} (r1 x r0): M's lower right block
     node_product(
         r1, r0, r0, -1.0, false, [&](int i, int k) { return W0s[i + k * r1]; },
-        [&](int k, int c) { return A[k * lda + src[c]]; },
+        [&](int k, int c) { return Ss[k + c * r0]; },
         [&](int i, int c, double v) { M[(r0 + i) + (long long)(r1 + c) * ldm] = TE(v); });
     __syncthreads();
     // I - V0Tu0 G0 (r1 x r1): M's lower left block
@@ -231,14 +297,14 @@ __global__ void __launch_bounds__(kNodeThreads)
   // F = -V0Tu0 S^{-1} (r1 x r0): M's lower right block and FP64 work copy
   node_product(
       r1, r0, r0, -1.0, false, [&](int i, int k) { return double(W0u[i + k * l0]); },
-      [&](int k, int c) { return A[k * lda + src[c]]; },
+      [&](int k, int c) { return A[at[k] * lda + src[c]]; },
       [&](int i, int c, double v) {
         F[i + (long long)c * r1] = v;
         M[(r0 + i) + (long long)(r1 + c) * ldm] = TE(v);
       });
   // G0 = -S^{-1} V1Tu1 (r0 x r1): M's upper left block
   node_product(
-      r0, r1, r0, -1.0, false, [&](int i, int k) { return A[i * lda + src[k]]; },
+      r0, r1, r0, -1.0, false, [&](int i, int k) { return A[at[i] * lda + src[k]]; },
       [&](int k, int c) { return double(W1u[k + c * l1]); },
       [&](int i, int c, double v) { M[i + (long long)c * ldm] = TE(v); });
   __syncthreads();  // F (global) visible to the whole CTA
@@ -258,13 +324,16 @@ void launch_node_factor(const NodeTask<TW, TE> *tasks, int count, int max_s, int
                         int *info, cudaStream_t s) {
   if (count <= 0) return;
   size_t smem = node_factor_smem(max_s);
-  const size_t staged = smem + 3 * (size_t)max_r * max_r * sizeof(double);
+  const size_t staged = smem + 4 * (size_t)max_r * max_r * sizeof(double);
   const int stage = (form == 0 && staged <= 200 * 1024) ? 1 : 0;
   if (stage) smem = staged;
-  HODLR_CUDA_TRY(cudaFuncSetAttribute(node_factor_kernel<TW, TE>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  node_factor_kernel<TW, TE><<<count, kNodeThreads, smem, s>>>(tasks, form, max_s, max_r, stage,
-                                                                info);
+  auto go = [&](auto kern) {
+    HODLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<count, kNodeThreads, smem, s>>>(tasks, form, max_s, max_r, stage, info);
+  };
+  if (max_s <= 32) go(node_factor_kernel<TW, TE, 1>);
+  else if (max_s <= 64) go(node_factor_kernel<TW, TE, 2>);
+  else go(node_factor_kernel<TW, TE, (kMaxNodeS + 31) / 32>);
   HODLR_LAUNCH_CHECK();
 }
 
