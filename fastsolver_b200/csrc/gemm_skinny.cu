@@ -312,12 +312,252 @@ __global__ void __launch_bounds__(kTNThreads)
   }
 }
 
+// ---------------------------------------------------------------- FP64 on the DMMA pipe
+// FP64 items of at most 16 columns (the HODLR matvec's D x + U t and V^T x)
+// run on the FP64 tensor-core instruction mma.m16n8k4.f64: one instruction
+// per 16 x 8 x 4 block instead of 512 FMAs, so the kernels stay bound by the
+// operand stream instead of by instruction issue.  Fragments (PTX layout of
+// m16n8k4 .f64, g = lane / 4, t = lane % 4): A a0 = A[g][t], a1 = A[g + 8][t];
+// B b = B[t][g]; C c0..c3 = C[g][2t], C[g][2t + 1], C[g + 8][2t], C[g + 8][2t + 1].
+__device__ inline void dmma(double (&c)[4], double a0, double a1, double b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, "
+      "{%0, %1, %2, %3};\n"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(b));
+}
+
+constexpr int kDmmaRows = 512;          // NN: 8 warps x 64 rows
+constexpr int kDmmaKT = 8;              // NN: K per stage
+constexpr int kDmmaStages = 3;
+constexpr int kDmmaAP = kDmmaRows + 8;  // padded k-row stride (doubles)
+
+// NN: C (M x N <= 16) = beta Cin + alpha sum_s A_s B_s, A_s column-major
+template <int NT8>
+__global__ void __launch_bounds__(kSkThreads, 2)
+    skinny_nn_dmma_kernel(const GemmItem<double, double> *__restrict__ items,
+                          const GemmSeg<double> *__restrict__ segs, double alpha, double beta) {
+  constexpr int KT = kDmmaKT, ROWS = kDmmaRows, AP = kDmmaAP, NCS = 8 * NT8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *As = reinterpret_cast<double *>(smem_raw);      // [stage][KT][AP]
+  double *Bs = As + (size_t)kDmmaStages * KT * AP;         // [stage][KT][NCS]
+  const GemmItem<double, double> it = items[blockIdx.x];
+  const int row0 = blockIdx.y * ROWS;
+  if (row0 >= it.M) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int N = it.N;
+
+  auto load = [&](const TileIter<double> &p, int st) {
+    if (p.valid) {
+      const GemmSeg<double> &sg = p.sg;
+      double *a = As + (size_t)st * KT * AP;
+      double *b = Bs + (size_t)st * KT * NCS;
+      const double *abase = sg.A + row0 + (long long)p.k0 * sg.lda;
+      const bool vec = ((reinterpret_cast<uintptr_t>(abase) & 15) == 0) && ((sg.lda & 1) == 0);
+      for (int e = tid; e < KT * (ROWS / 2); e += kSkThreads) {
+        const int k = e / (ROWS / 2), rv = e % (ROWS / 2);
+        const int r = row0 + 2 * rv;
+        const bool kin = p.k0 + k < sg.K;
+        const double *src = abase + 2 * rv + (long long)k * sg.lda;
+        double *dst = a + k * AP + 2 * rv;
+        if (vec && kin && r + 2 <= it.M) {
+          cpa(dst, src, 16, true);
+        } else {
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const bool ok = kin && r + u < it.M;
+            cpa(dst + u, ok ? src + u : sg.A, 8, ok);
+          }
+        }
+      }
+      for (int e = tid; e < KT * NCS; e += kSkThreads) {
+        const int k = e % KT, n = e / KT;
+        const bool ok = (p.k0 + k < sg.K) && n < N;
+        cpa(b + k * NCS + n, ok ? sg.B + (p.k0 + k) + (long long)n * sg.ldb : sg.B, 8, ok);
+      }
+    }
+    cpa_commit();
+  };
+
+  double acc[4][NT8][4];
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < NT8; ++nt)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[mt][nt][v] = 0.0;
+  TileIter<double> ld, cp;
+  ld.init(segs, it.seg_begin, it.seg_count);
+  cp = ld;
+#pragma unroll
+  for (int i = 0; i < kDmmaStages - 1; ++i) {
+    load(ld, i);
+    if (ld.valid) ld.next(KT);
+  }
+  int st = 0, lst = kDmmaStages - 1;
+  const int wrow = warp * 64;
+  while (cp.valid) {
+    load(ld, lst);
+    if (ld.valid) ld.next(KT);
+    lst = (lst + 1) % kDmmaStages;
+    cpa_wait<kDmmaStages - 1>();
+    __syncthreads();
+    const double *a = As + (size_t)st * KT * AP;
+    const double *b = Bs + (size_t)st * KT * NCS;
+#pragma unroll
+    for (int ks = 0; ks < KT; ks += 4) {
+      const double *ak = a + (ks + t) * AP + wrow + g;
+      double bv[NT8];
+#pragma unroll
+      for (int nt = 0; nt < NT8; ++nt) bv[nt] = b[(ks + t) * NCS + nt * 8 + g];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        const double a0 = ak[mt * 16], a1 = ak[mt * 16 + 8];
+#pragma unroll
+        for (int nt = 0; nt < NT8; ++nt) dmma(acc[mt][nt], a0, a1, bv[nt]);
+      }
+    }
+    __syncthreads();  // stage st is refilled kDmmaStages - 1 tiles later
+    st = (st + 1) % kDmmaStages;
+    cp.next(KT);
+  }
+  cpa_wait<0>();
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < NT8; ++nt)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int row = row0 + wrow + mt * 16 + g + (v >> 1) * 8;
+        const int col = nt * 8 + 2 * t + (v & 1);
+        if (row < it.M && col < N) {
+          double val = alpha * acc[mt][nt][v];
+          if (it.Cin) val += beta * it.Cin[row + (long long)col * it.ldcin];
+          it.C[row + (long long)col * it.ldc] = val;
+        }
+      }
+}
+
+// TN: C (64 x 16 block of an item, over all K) = beta Cin + alpha sum_s A_s^T B_s
+constexpr int kDmmaKC = 32;
+constexpr int kDmmaLDK = kDmmaKC + 4;  // padded k stride (doubles): conflict-free fragments
+
+__global__ void __launch_bounds__(kTNThreads)
+    skinny_tn_dmma_kernel(const GemmItem<double, double> *__restrict__ items,
+                          const GemmSeg<double> *__restrict__ segs, double alpha, double beta) {
+  constexpr int TM = 64, TN = 16, KC = kDmmaKC, LDK = kDmmaLDK;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *As = reinterpret_cast<double *>(smem_raw);   // [stage][TM][LDK]
+  double *Bs = As + (size_t)kSkStages * TM * LDK;      // [stage][TN][LDK]
+  const GemmItem<double, double> it = items[blockIdx.x];
+  const int m0 = blockIdx.y * TM, n0 = blockIdx.z * TN;
+  if (m0 >= it.M || n0 >= it.N) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+
+  auto load_block = [&](double *dst, const double *base, long long ld, int k0, int K, int c0,
+                        int ncols, int cmax) {
+    const double *p0 = base + k0 + (long long)c0 * ld;
+    const bool vec = ((reinterpret_cast<uintptr_t>(p0) & 15) == 0) && ((ld & 1) == 0);
+    for (int e = tid; e < ncols * (KC / 2); e += kTNThreads) {
+      const int c = e / (KC / 2), kv = e % (KC / 2);
+      const int k = k0 + 2 * kv;
+      const bool colok = c0 + c < cmax;
+      const double *src = p0 + 2 * kv + (long long)c * ld;
+      double *d = dst + c * LDK + 2 * kv;
+      if (vec && colok && k + 2 <= K) {
+        cpa(d, src, 16, true);
+      } else {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const bool ok = colok && k + u < K;
+          cpa(d + u, ok ? src + u : base, 8, ok);
+        }
+      }
+    }
+  };
+  auto load = [&](const TileIter<double> &p, int st) {
+    if (p.valid) {
+      load_block(As + (size_t)st * TM * LDK, p.sg.A, p.sg.lda, p.k0, p.sg.K, m0, TM, it.M);
+      load_block(Bs + (size_t)st * TN * LDK, p.sg.B, p.sg.ldb, p.k0, p.sg.K, n0, TN, it.N);
+    }
+    cpa_commit();
+  };
+
+  double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+  TileIter<double> ld, cp;
+  ld.init(segs, it.seg_begin, it.seg_count);
+  cp = ld;
+#pragma unroll
+  for (int i = 0; i < kSkStages - 1; ++i) {
+    load(ld, i);
+    if (ld.valid) ld.next(KC);
+  }
+  int st = 0, lst = kSkStages - 1;
+  while (cp.valid) {
+    load(ld, lst);
+    if (ld.valid) ld.next(KC);
+    lst = (lst + 1) % kSkStages;
+    cpa_wait<kSkStages - 1>();
+    __syncthreads();
+    const double *a = As + (size_t)st * TM * LDK + (warp * 16 + g) * LDK + t;
+    const double *b = Bs + (size_t)st * TN * LDK + g * LDK + t;
+#pragma unroll
+    for (int ks = 0; ks < KC; ks += 4) {
+      const double a0 = a[ks], a1 = a[8 * LDK + ks];
+      dmma(acc[0], a0, a1, b[ks]);
+      dmma(acc[1], a0, a1, b[8 * LDK + ks]);
+    }
+    __syncthreads();
+    st = (st + 1) % kSkStages;
+    cp.next(KC);
+  }
+  cpa_wait<0>();
+#pragma unroll
+  for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int gm = m0 + warp * 16 + g + (v >> 1) * 8;
+      const int gn = n0 + nt * 8 + 2 * t + (v & 1);
+      if (gm < it.M && gn < it.N) {
+        double val = alpha * acc[nt][v];
+        if (it.Cin) val += beta * it.Cin[gm + (long long)gn * it.ldcin];
+        it.C[gm + (long long)gn * it.ldc] = val;
+      }
+    }
+}
+
 }  // namespace
 
 template <typename T>
 void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nitems, int max_m,
                    int max_n, bool trans, T alpha, T beta, cudaStream_t s) {
   if (nitems <= 0 || max_m <= 0 || max_n <= 0) return;
+  if constexpr (sizeof(T) == 8) {
+    if (max_n <= 16) {
+      if (trans) {
+        const size_t smem = (size_t)kSkStages * (64 + 16) * kDmmaLDK * sizeof(double);
+        HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_tn_dmma_kernel,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        dim3 grid(nitems, cdiv(max_m, 64), cdiv(max_n, 16));
+        skinny_tn_dmma_kernel<<<grid, kTNThreads, smem, s>>>(items, segs, alpha, beta);
+      } else {
+        dim3 grid(nitems, cdiv(max_m, kDmmaRows));
+        auto go = [&](auto kern, int ncs) {
+          const size_t smem =
+              (size_t)kDmmaStages * kDmmaKT * (kDmmaAP + ncs) * sizeof(double);
+          HODLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+          kern<<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);
+        };
+        if (max_n <= 8) go(skinny_nn_dmma_kernel<1>, 8);
+        else go(skinny_nn_dmma_kernel<2>, 16);
+      }
+      HODLR_LAUNCH_CHECK();
+      return;
+    }
+  }
   if (trans) {
     constexpr int TM = 64, TN = 16, KC = 32, LDK = KC + 16 / sizeof(T);
     const size_t smem = (size_t)kSkStages * (TM + TN) * LDK * sizeof(T);
