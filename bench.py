@@ -311,7 +311,10 @@ def main():
     def max_over_ranks(x: float) -> float:
         return rank_max(x, dist, "cuda")
 
-    stream = torch.cuda.current_stream()
+    # a side stream: the solve's replayable segments are captured as CUDA
+    # graphs on their first call (the legacy default stream cannot be captured)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     h = make_system(fs, cfg, args.seed + rank)
     tree = h.tree_nodes()
     solver = fs.FastSolver()

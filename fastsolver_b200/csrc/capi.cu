@@ -19,6 +19,8 @@ thread_local long long g_launches = 0;
 }
 
 void count_launch() { ++g_launches; }
+void add_launches(long long n) { g_launches += n; }
+long long launch_total() { return g_launches; }
 
 }  // namespace hodlr
 
@@ -713,8 +715,13 @@ int hodlr_solve_fused(hodlr_system h, int schur2, int sync, hodlr_stream_t strea
   if (schur2 && 2 * h->sys.r > kMaxNodeS) return HODLR_ERR_UNSUPPORTED;
   return guarded([&]() -> int {
     cudaStream_t s = as_stream(stream);
-    h->sys.run_fused64(schur2 ? 1 : 0, s);
-    if (sync) return h->sys.check_info(s);
+    System &S = h->sys;
+    const int form = schur2 ? 1 : 0;
+    S.ensure_fp64();
+    S.run_graph(S.g_fused64[form], s, [&]() { S.run_fused64(form, s); });
+    S.factored = HODLR_PREC_FP64;
+    S.factored_form = form;
+    if (sync) return S.check_info(s);
     return 0;
   });
 }
@@ -761,29 +768,49 @@ int hodlr_solve_refined(hodlr_system h, int precision, double tol, int maxiter, 
     cudaStream_t s = as_stream(stream);
     const long long N = S.N;
     const size_t nm = (size_t)N * S.m;
+    // two replayable segments: factor pass + residual, and one refinement
+    // sweep + residual (captured as CUDA graphs on the first call)
     if (precision == HODLR_PREC_MIXED) {
-      S.run_factor32(s);
-      launch_convert2d<float, double>(S.X32.p, N, S.Xsol.p, N, N, S.m, s);
+      S.ensure_mixed();
+      S.run_graph(S.g_factor32, s, [&]() {
+        S.run_factor32(s);
+        launch_convert2d<float, double>(S.X32.p, N, S.Xsol.p, N, N, S.m, s);
+        S.relres_enqueue(s);
+      });
+      S.factored = HODLR_PREC_MIXED;  // (host state is not part of a replay)
+      S.factored_form = 0;
     } else {
-      S.run_fused64(0, s);
+      S.ensure_fp64();
+      S.run_graph(S.g_factor64, s, [&]() {
+        S.run_fused64(0, s);
+        S.relres_enqueue(s);
+      });
+      S.factored = HODLR_PREC_FP64;
+      S.factored_form = 0;
     }
     int info = S.check_info(s);
     if (info) return info;
     int it = 0;
-    double rr = S.relres(s);
+    double rr = S.relres_read(s);
     while (rr > tol && it < maxiter) {
       if (precision == HODLR_PREC_MIXED) {
-        launch_convert2d<double, float>(S.R64.p, N, S.Y32.p, N, N, S.m, s);
-        S.run_apply32(s);
-        launch_add2d<float>(S.Xsol.p, N, S.Y32.p, N, N, S.m, s);
+        S.run_graph(S.g_sweep32, s, [&]() {
+          launch_convert2d<double, float>(S.R64.p, N, S.Y32.p, N, N, S.m, s);
+          S.run_apply32(s);
+          launch_add2d<float>(S.Xsol.p, N, S.Y32.p, N, N, S.m, s);
+          S.relres_enqueue(s);
+        });
       } else {
-        HODLR_CUDA_TRY(cudaMemcpyAsync(S.Y64.p, S.R64.p, sizeof(double) * nm,
-                                       cudaMemcpyDeviceToDevice, s));
-        S.run_apply64(s);
-        launch_add2d<double>(S.Xsol.p, N, S.Y64.p, N, N, S.m, s);
+        S.run_graph(S.g_sweep64, s, [&]() {
+          HODLR_CUDA_TRY(cudaMemcpyAsync(S.Y64.p, S.R64.p, sizeof(double) * nm,
+                                         cudaMemcpyDeviceToDevice, s));
+          S.run_apply64(s);
+          launch_add2d<double>(S.Xsol.p, N, S.Y64.p, N, N, S.m, s);
+          S.relres_enqueue(s);
+        });
       }
       ++it;
-      rr = S.relres(s);
+      rr = S.relres_read(s);
     }
     if (iters) *iters = it;
     if (relres) *relres = rr;

@@ -15,6 +15,8 @@ namespace hodlr {
 // ---------------------------------------------------------------------------
 
 void count_launch();  // one per kernel launch issued by the library
+void add_launches(long long n);  // launches replayed by a CUDA graph
+long long launch_total();
 
 struct CudaError {
   cudaError_t err;

@@ -800,9 +800,17 @@ int System::check_info(cudaStream_t s) {
   return 0;
 }
 
-double System::relres(cudaStream_t s) {
+void System::relres_enqueue(cudaStream_t s) {
   run_matvec(mv_sol, -1.0, 1.0, s);
   launch_colratio(R64.p, N, B.p, N, N, m, relres_dev.p, s);
+}
+
+double System::relres(cudaStream_t s) {
+  relres_enqueue(s);
+  return relres_read(s);
+}
+
+double System::relres_read(cudaStream_t s) {
   std::vector<double> h(m);
   HODLR_CUDA_TRY(cudaMemcpyAsync(h.data(), relres_dev.p, sizeof(double) * m,
                                  cudaMemcpyDeviceToHost, s));

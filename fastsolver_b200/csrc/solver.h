@@ -156,6 +156,21 @@ struct Profiler {
   void reset();
 };
 
+// A replayable segment of the solve captured once as a CUDA graph.  The
+// segment only depends on the system's buffers (fixed after the first solve),
+// so the captured graph stays valid for every later right-hand side or
+// matrix loaded into the same buffers.
+struct GraphSeg {
+  cudaGraphExec_t exec = nullptr;
+  long long kernels = 0;  // kernel launches recorded in the graph
+  GraphSeg() = default;
+  GraphSeg(const GraphSeg &) = delete;
+  GraphSeg &operator=(const GraphSeg &) = delete;
+  ~GraphSeg() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
 struct System {
   Tree tree;
   int N = 0, m = 0, r = 0, C = 0, vc = 0, nmax = 0;
@@ -183,6 +198,8 @@ struct System {
   int bc_chunk = 512;
   int n_info = 0;
   Profiler prof;
+  bool use_graphs = true;  // replay captured segments (off while profiling)
+  GraphSeg g_factor32, g_sweep32, g_factor64, g_fused64[2], g_sweep64;
 
   int init(int N_, int nrhs, int rank, int threshold);
   void ensure_fp64();
@@ -195,6 +212,41 @@ struct System {
   void run_matvec(const MatvecPlan &p, double alpha, double beta, cudaStream_t s);
   int check_info(cudaStream_t s);                 // sync + first nonzero INFO
   double relres(cudaStream_t s);                  // of Xsol against B (sync)
+  void relres_enqueue(cudaStream_t s);            // matvec + column ratios into relres_dev
+  double relres_read(cudaStream_t s);             // sync + max of relres_dev
+  // Runs `fn` (stream work on s) through the graph cache `g`: captured on the
+  // first call, replayed afterwards; eager when graphs are off, while
+  // profiling, or on the legacy default stream (which cannot be captured).
+  template <typename F>
+  void run_graph(GraphSeg &g, cudaStream_t s, F &&fn) {
+    if (!use_graphs || prof.on || s == nullptr) {
+      fn();
+      return;
+    }
+    if (!g.exec) {
+      const long long before = launch_total();
+      cudaGraph_t graph = nullptr;
+      HODLR_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      try {
+        fn();
+      } catch (...) {
+        cudaStreamEndCapture(s, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+      }
+      HODLR_CUDA_TRY(cudaStreamEndCapture(s, &graph));
+      cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        g.exec = nullptr;
+        throw CudaError{e};
+      }
+      g.kernels = launch_total() - before;
+      add_launches(-g.kernels);  // counted when replayed
+    }
+    HODLR_CUDA_TRY(cudaGraphLaunch(g.exec, s));
+    add_launches(g.kernels);
+  }
 };
 
 }  // namespace hodlr

@@ -163,3 +163,37 @@ def test_save_solution_reference_format(fs, cuda, tmp_path):
     assert len(rows) == 480
     vals = np.array([[float(v) for v in r.split("\t") if v] for r in rows])
     np.testing.assert_array_equal(vals, h.solution())
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_graph_replay_new_rhs(fs, oracle, cuda, precision):
+    """On a side stream the refined solve is captured as CUDA graphs on its
+    first call and replayed afterwards: a second right-hand side loaded into
+    the same system must be solved as accurately as the first, and the fused
+    FP64 solve replayed on a third one must match the oracle."""
+    import torch
+    N, m, r, t = 8192, 3, 20, 256
+    s = make_gauss(oracle, N, m, r, t, seed=11)
+    h = gpu_system(fs, s)
+    prec = fs.PREC_MIXED if precision == "mixed" else fs.PREC_FP64
+    st = torch.cuda.Stream()
+    sol = fs.FastSolver()
+    rng = np.random.default_rng(5)
+    for trial in range(3):
+        B = np.asfortranarray(rng.standard_normal((N, m)))
+        h.set_rhs(B, stream=st)
+        s.B = B
+        it, rr = sol.solve_refined(h, prec, tol=1e-12, maxiter=10, stream=st)
+        st.synchronize()
+        assert rr <= 1e-12, (trial, rr)
+        x = h.solution(stream=st)
+        Xo, _ = oracle.bfs_solve(s, nthreads=8)
+        assert relerr(x, Xo[:, :m]) < 1e-11
+    for trial in range(2):
+        B = np.asfortranarray(rng.standard_normal((N, m)))
+        h.set_rhs(B, stream=st)
+        s.B = B
+        sol.bfs_solve(h, stream=st)
+        st.synchronize()
+        Xo, _ = oracle.bfs_solve(s, nthreads=8)
+        assert relerr(h.solution(stream=st), Xo[:, :m]) < 1e-12
