@@ -76,6 +76,11 @@ _SIGS = {
     "hodlr_get_solution": [_vp, _vp, _ll, _i, _vp],
     "hodlr_set_profiling": [_vp, _i],
     "hodlr_phase_times": [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), _i],
+    "hodlr_batch_create": [ctypes.POINTER(_vp), ctypes.POINTER(_vp), _i],
+    "hodlr_batch_destroy": [_vp],
+    "hodlr_batch_solve_refined": [_vp, _d, _i, _ip, _dp, _dp, _ip, _vp],
+    "hodlr_batch_set_profiling": [_vp, _i],
+    "hodlr_batch_phase_times": [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), _i],
     "hodlr_launch_count": [],
     "hodlr_reset_launch_count": [],
     "hodlr_status_string": [_i],

@@ -30,6 +30,10 @@ struct hodlr_system_s {
   System sys;
 };
 
+struct hodlr_batch_s {
+  Batch b;
+};
+
 namespace {
 
 // Runs `f` and maps library exceptions to status codes.
@@ -847,6 +851,90 @@ int hodlr_set_profiling(hodlr_system h, int on) {
 }
 
 static_assert(PH_COUNT == HODLR_PHASES, "phase list of the C ABI");
+
+int hodlr_batch_create(hodlr_batch *out, const hodlr_system *systems, int count) {
+  if (!out) return -1;
+  *out = nullptr;
+  if (!systems) return -2;
+  if (count <= 0 || count > 16384) return -3;
+  for (int k = 0; k < count; ++k)
+    if (!systems[k]) return -2;
+  if (int rc = device_ok()) return rc;
+  return guarded([&]() -> int {
+    auto *h = new hodlr_batch_s();
+    try {
+      std::vector<System *> v;
+      for (int k = 0; k < count; ++k) v.push_back(&systems[k]->sys);
+      h->b.build(v);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return 0;
+  });
+}
+
+int hodlr_batch_destroy(hodlr_batch batch) {
+  if (!batch) return -1;
+  delete batch;
+  return 0;
+}
+
+int hodlr_batch_solve_refined(hodlr_batch batch, double tol, int maxiter, int *iters,
+                              double *relres_max, double *relres, int *failed,
+                              hodlr_stream_t stream) {
+  if (!batch) return -1;
+  if (!(tol >= 0.0)) return -2;
+  if (maxiter < 0) return -3;
+  return guarded([&]() -> int {
+    Batch &B = batch->b;
+    cudaStream_t s = as_stream(stream);
+    B.run_graph(B.g_factor, s, [&]() { B.run_factor(s); });
+    for (System *S : B.sys) {
+      S->factored = HODLR_PREC_MIXED;
+      S->factored_form = 0;
+    }
+    int info = B.check_info(s, failed);
+    if (info) return info;
+    std::vector<double> per;
+    int it = 0;
+    double rr = B.relres_read(s, &per);
+    while (rr > tol && it < maxiter) {
+      B.run_graph(B.g_sweep, s, [&]() { B.run_sweep(s); });
+      ++it;
+      rr = B.relres_read(s, &per);
+    }
+    if (iters) *iters = it;
+    if (relres_max) *relres_max = rr;
+    if (relres)
+      for (size_t k = 0; k < per.size(); ++k) relres[k] = per[k];
+    return rr <= tol ? 0 : HODLR_ERR_NOCONV;
+  });
+}
+
+int hodlr_batch_set_profiling(hodlr_batch batch, int on) {
+  if (!batch) return -1;
+  return guarded([&]() -> int {
+    batch->b.prof.reset();
+    batch->b.prof.on = on != 0;
+    return 0;
+  });
+}
+
+int hodlr_batch_phase_times(hodlr_batch batch, double *ms, long long *launches, int reset) {
+  if (!batch) return -1;
+  return guarded([&]() -> int {
+    Profiler &p = batch->b.prof;
+    p.collect();
+    for (int i = 0; i < PH_COUNT; ++i) {
+      if (ms) ms[i] = p.ms[i];
+      if (launches) launches[i] = p.launches[i];
+    }
+    if (reset) p.reset();
+    return 0;
+  });
+}
 
 int hodlr_phase_times(hodlr_system h, double *ms, long long *launches, int reset) {
   if (!h) return -1;

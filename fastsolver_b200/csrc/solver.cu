@@ -46,6 +46,7 @@ struct PathSpec {
   TE *M = nullptr;     // per-node solve matrices, (2r)^2 each
   NodeStore *ns = nullptr;
   const LeafPlan<T> *factors = nullptr;  // apply paths: the blocked leaf factors
+  int nb_force = 0;                      // leaf panel width (0: by the largest leaf)
   bool factor = false;
   int red_chunk = 512, bc_chunk = 512;
 };
@@ -86,12 +87,13 @@ void path_need(const Tree &t, bool factor, int chunk, size_t &part, size_t &wfin
 // leaf_blocked.cu): forward steps on [D | X], then the backward solve on X.
 template <typename T>
 void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long ldx,
-                     int *ipiv, int *perm, bool factor_cols_all, int m, LeafPlan<T> &lp) {
+                     int *ipiv, int *perm, bool factor_cols_all, int m, LeafPlan<T> &lp,
+                     int nb_force) {
   const int nleaf = (int)t.leaves.size();
   int max_panels = 0;
   lp.max_n = 0;
   for (int id : t.leaves) lp.max_n = std::max(lp.max_n, t.nodes[id].nrow);
-  const int NB = leaf_nb<T>(lp.max_n);
+  const int NB = nb_force > 0 ? nb_force : leaf_nb<T>(lp.max_n);
   lp.nb = NB;
   for (int id : t.leaves) max_panels = std::max(max_panels, cdiv(t.nodes[id].nrow, NB));
   lp.Linv.ensure((size_t)nleaf * max_panels * NB * NB);
@@ -225,7 +227,8 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
   plan.nleaf = (int)lt.size();
   plan.leaf_tasks.upload(lt);
   if (sp.factor) {
-    build_leaf_plan<T>(t, sp.D, sp.ldd, sp.X, sp.ldx, sp.ipiv, sp.perm, true, m, plan.leaf);
+    build_leaf_plan<T>(t, sp.D, sp.ldd, sp.X, sp.ldx, sp.ipiv, sp.perm, true, m, plan.leaf,
+                       sp.nb_force);
   } else if (sp.factors) {
     std::vector<LeafFactorTask<T>> at = sp.factors->host_tasks;
     for (size_t q = 0; q < at.size(); ++q) {
@@ -626,6 +629,186 @@ void build_matvec(System &S, const double *x, MatvecPlan &mv) {
   mv.built = true;
 }
 
+// ---- merging the plans of several systems into one batch schedule.  All
+// descriptors hold absolute device pointers into their own system's buffers,
+// so merging is concatenation: item lists shift their segment indices, INFO
+// slots shift by the system's offset in the batch's INFO array.
+
+template <typename TA, typename TC>
+struct ItemAcc {
+  std::vector<GemmItem<TA, TC>> it;
+  std::vector<GemmSeg<TA>> sg;
+  int max_m = 0, max_n = 0;
+  void add(const std::vector<GemmItem<TA, TC>> &items, const std::vector<GemmSeg<TA>> &segs) {
+    const int off = (int)sg.size();
+    for (GemmItem<TA, TC> x : items) {
+      x.seg_begin += off;
+      it.push_back(x);
+      max_m = std::max(max_m, x.M);
+      max_n = std::max(max_n, x.N);
+    }
+    sg.insert(sg.end(), segs.begin(), segs.end());
+  }
+  void add(const GemmLaunch<TA, TC> &g) { add(g.items.h, g.segs.h); }
+  void store(GemmLaunch<TA, TC> &g) const { g.set(it, sg); }
+  void store(DevBuf<GemmItem<TA, TC>> &items, DevBuf<GemmSeg<TA>> &segs, int &n, int &mm,
+             int &mn) const {
+    items.upload(it);
+    segs.upload(sg);
+    n = (int)it.size();
+    mm = max_m;
+    mn = max_n;
+  }
+};
+
+template <typename T>
+void merge_leaf_plans(const std::vector<const LeafPlan<T> *> &src, const std::vector<int> &info_off,
+                      LeafPlan<T> &dst) {
+  std::vector<LeafFactorTask<T>> tasks;
+  dst.max_n = dst.laswp_cols = 0;
+  dst.nb = src.empty() ? 0 : src[0]->nb;
+  size_t panels = 0;
+  for (size_t k = 0; k < src.size(); ++k) {
+    const LeafPlan<T> &lp = *src[k];
+    if (lp.nb != dst.nb) throw CudaError{cudaErrorInvalidValue};
+    for (LeafFactorTask<T> t : lp.host_tasks) {
+      t.info_slot += info_off[k];
+      tasks.push_back(t);
+    }
+    dst.max_n = std::max(dst.max_n, lp.max_n);
+    dst.laswp_cols = std::max(dst.laswp_cols, lp.laswp_cols);
+    panels = std::max(panels, lp.fwd.size());
+  }
+  dst.tasks.upload(tasks);
+  dst.host_tasks = tasks;
+  dst.nleaf = (int)tasks.size();
+  dst.fwd.clear();
+  dst.bwd.clear();
+  for (size_t pi = 0; pi < panels; ++pi) {
+    auto F = std::make_unique<typename LeafPlan<T>::Fwd>();
+    F->k0 = (int)pi * dst.nb;
+    F->panel = (int)pi;
+    ItemAcc<T, T> tr, up;
+    for (const LeafPlan<T> *lp : src) {
+      if (pi >= lp->fwd.size()) continue;
+      tr.add(lp->fwd[pi]->trsm);
+      up.add(lp->fwd[pi]->update);
+    }
+    tr.store(F->trsm);
+    up.store(F->update);
+    dst.fwd.push_back(std::move(F));
+  }
+  // backward steps run from the last panel to the first; a system's bwd[j]
+  // is its panel fwd.size() - 1 - j
+  for (size_t j = 0; j < panels; ++j) {
+    const size_t pi = panels - 1 - j;
+    auto B = std::make_unique<typename LeafPlan<T>::Bwd>();
+    ItemAcc<T, T> tr, up;
+    for (const LeafPlan<T> *lp : src) {
+      if (pi >= lp->fwd.size()) continue;
+      const size_t jj = lp->fwd.size() - 1 - pi;
+      tr.add(lp->bwd[jj]->trsm);
+      up.add(lp->bwd[jj]->update);
+    }
+    tr.store(B->trsm);
+    up.store(B->update);
+    dst.bwd.push_back(std::move(B));
+  }
+}
+
+// Level j of the merged plan is level j (deepest first) of every system
+// that has one: each system still walks its own levels bottom-up.
+template <typename T, typename TE>
+void merge_paths(const std::vector<const PathPlan<T, TE> *> &src, const std::vector<int> &info_off,
+                 PathPlan<T, TE> &dst) {
+  dst.levels.clear();
+  dst.factor = src[0]->factor;
+  dst.nleaf = 0;
+  dst.max_n = dst.max_nrhs = 0;
+  dst.apply_nb = dst.apply_max_n = dst.apply_max_cols = 0;
+  if (dst.factor) {
+    std::vector<const LeafPlan<T> *> lps;
+    for (const auto *p : src) lps.push_back(&p->leaf);
+    merge_leaf_plans<T>(lps, info_off, dst.leaf);
+    dst.nleaf = dst.leaf.nleaf;
+  } else {
+    std::vector<LeafFactorTask<T>> at;
+    for (const auto *p : src) {
+      at.insert(at.end(), p->apply_tasks.h.begin(), p->apply_tasks.h.end());
+      if (p->apply_nb != src[0]->apply_nb) throw CudaError{cudaErrorInvalidValue};
+      dst.apply_max_n = std::max(dst.apply_max_n, p->apply_max_n);
+      dst.apply_max_cols = std::max(dst.apply_max_cols, p->apply_max_cols);
+    }
+    dst.apply_tasks.upload(at);
+    dst.apply_nb = src[0]->apply_nb;
+    dst.nleaf = (int)at.size();
+  }
+  size_t nlev = 0;
+  for (const auto *p : src) nlev = std::max(nlev, p->levels.size());
+  for (size_t j = 0; j < nlev; ++j) {
+    auto L = std::make_unique<LevelPlan<T, TE>>();
+    ItemAcc<T, T> red, ap, bc;
+    ItemAcc<T, double> gram;
+    std::vector<SumTask<T>> su;
+    std::vector<NodeTask<T, TE>> nt;
+    for (size_t k = 0; k < src.size(); ++k) {
+      if (j >= src[k]->levels.size()) continue;
+      const LevelPlan<T, TE> &S = *src[k]->levels[j];
+      red.add(S.red_items.h, S.red_segs.h);
+      gram.add(S.gram_items.h, S.gram_segs.h);
+      ap.add(S.ap_items.h, S.ap_segs.h);
+      bc.add(S.bc_items.h, S.bc_segs.h);
+      su.insert(su.end(), S.sums.h.begin(), S.sums.h.end());
+      L->sum_max_len = std::max(L->sum_max_len, S.sum_max_len);
+      for (NodeTask<T, TE> t : S.node_tasks.h) {
+        t.info_slot += info_off[k];
+        nt.push_back(t);
+      }
+      L->max_s = std::max(L->max_s, S.max_s);
+      L->max_r = std::max(L->max_r, S.max_r);
+    }
+    red.store(L->red_items, L->red_segs, L->n_red, L->red_max_m, L->red_max_n);
+    int gm = 0, gn = 0;
+    gram.store(L->gram_items, L->gram_segs, L->n_gram, gm, gn);
+    L->gram_max = std::max(gm, gn);
+    ap.store(L->ap_items, L->ap_segs, L->n_ap, L->ap_max_m, L->ap_max_n);
+    bc.store(L->bc_items, L->bc_segs, L->n_bc, L->bc_max_m, L->bc_max_n);
+    L->sums.upload(su);
+    L->n_sums = (int)su.size();
+    L->node_tasks.upload(nt);
+    L->n_nodes = (int)nt.size();
+    dst.levels.push_back(std::move(L));
+  }
+  dst.built = true;
+}
+
+void merge_matvecs(const std::vector<const MatvecPlan *> &src, MatvecPlan &dst) {
+  ItemAcc<double, double> red, ap;
+  std::vector<SumTask<double>> su;
+  dst.sum_max_len = 0;
+  for (const MatvecPlan *p : src) {
+    red.add(p->red_items.h, p->red_segs.h);
+    ap.add(p->ap_items.h, p->ap_segs.h);
+    su.insert(su.end(), p->sums.h.begin(), p->sums.h.end());
+    dst.sum_max_len = std::max(dst.sum_max_len, p->sum_max_len);
+  }
+  red.store(dst.red_items, dst.red_segs, dst.n_red, dst.red_max_m, dst.red_max_n);
+  ap.store(dst.ap_items, dst.ap_segs, dst.n_ap, dst.ap_max_m, dst.ap_max_n);
+  dst.sums.upload(su);
+  dst.n_sums = (int)su.size();
+  dst.built = true;
+}
+
+void matvec_launches(Profiler &pf, const MatvecPlan &p, double alpha, double beta,
+                     cudaStream_t s) {
+  PhaseScope ps(pf, PH_MATVEC, s);
+  launch_gemm_items<double, double, double>(p.red_items.p, p.red_segs.p, p.n_red, p.red_max_m,
+                                            p.red_max_n, true, 1.0, 0.0, s);
+  launch_sum_slots<double>(p.sums.p, p.n_sums, p.sum_max_len, s);
+  launch_gemm_items<double, double, double>(p.ap_items.p, p.ap_segs.p, p.n_ap, p.ap_max_m,
+                                            p.ap_max_n, false, alpha, beta, s);
+}
+
 }  // namespace
 
 void Profiler::begin(int ph, cudaStream_t s, cudaEvent_t &a) {
@@ -737,7 +920,7 @@ void System::ensure_mixed() {
   f.X = X32.p; f.ldx = N; f.Usrc = X32.p; f.ldu = N;
   f.D = D32.p; f.ldd = N; f.ipiv = ipiv32.p; f.perm = perm32.p;
   f.V = V32.p; f.ldv = N; f.part = part32.p; f.wfin = wfin32.p; f.eta = eta32.p; f.M = ns32.M32.p; f.ns = &ns32;
-  f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk;
+  f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk; f.nb_force = nb32;
   build_path(tree, f, fused32, 0);
   PathSpec<float, float> a = f;
   a.X = Y32.p; a.factor = false; a.factors = &fused32.leaf;
@@ -763,6 +946,13 @@ void System::run_apply64(cudaStream_t s) {
 }
 
 void System::run_factor32(cudaStream_t s) {
+  convert32(s);
+  run_path(prof, fused32, 0, info.p, s);
+  factored = HODLR_PREC_MIXED;
+  factored_form = 0;
+}
+
+void System::convert32(cudaStream_t s) {
   ensure_mixed();
   const long long n = N;
   {
@@ -774,20 +964,12 @@ void System::run_factor32(cudaStream_t s) {
       launch_convert2d<double, float>(V.p, n, V32.p, n, n, vc, s);
     }
   }
-  run_path(prof, fused32, 0, info.p, s);
-  factored = HODLR_PREC_MIXED;
-  factored_form = 0;
 }
 
 void System::run_apply32(cudaStream_t s) { run_path(prof, apply32, 0, nullptr, s); }
 
 void System::run_matvec(const MatvecPlan &p, double alpha, double beta, cudaStream_t s) {
-  PhaseScope ps(prof, PH_MATVEC, s);
-  launch_gemm_items<double, double, double>(p.red_items.p, p.red_segs.p, p.n_red, p.red_max_m,
-                                            p.red_max_n, true, 1.0, 0.0, s);
-  launch_sum_slots<double>(p.sums.p, p.n_sums, p.sum_max_len, s);
-  launch_gemm_items<double, double, double>(p.ap_items.p, p.ap_segs.p, p.n_ap, p.ap_max_m,
-                                            p.ap_max_n, false, alpha, beta, s);
+  matvec_launches(prof, p, alpha, beta, s);
 }
 
 int System::check_info(cudaStream_t s) {
@@ -817,6 +999,144 @@ double System::relres_read(cudaStream_t s) {
   HODLR_CUDA_TRY(cudaStreamSynchronize(s));
   double mx = 0.0;
   for (double v : h) mx = std::max(mx, std::isnan(v) ? INFINITY : v);
+  return mx;
+}
+
+// ---- Batch
+
+void Batch::build(const std::vector<System *> &systems) {
+  if (systems.empty()) throw CudaError{cudaErrorInvalidValue};
+  sys = systems;
+  // one FP32 leaf panel width for all: the merged panel launches share it
+  int gmax = 0;
+  for (System *S : sys) gmax = std::max(gmax, S->nmax);
+  nb = leaf_nb<float>(gmax);
+  for (System *S : sys) {
+    if (S->fused32.built && S->fused32.leaf.nb != nb) {
+      S->fused32.built = false;  // rebuild the plans with the common width
+      S->reset_graphs();
+    }
+    S->nb32 = nb;
+    S->ensure_mixed();
+  }
+  info_off.clear();
+  rr_off.clear();
+  n_info = 0;
+  int n_rr = 0;
+  max_m = 0;
+  std::vector<const PathPlan<float, float> *> fp, ap;
+  std::vector<const MatvecPlan *> mp;
+  std::vector<Ew2DTask<double, float>> cin, cres;
+  std::vector<Ew2DTask<float, double>> cx0, addy;
+  std::vector<RatioTask> rt;
+  t_in = t_res = t_x0 = 0;
+  for (System *S : sys) {
+    info_off.push_back(n_info);
+    n_info += S->n_info;
+    rr_off.push_back(n_rr);
+    n_rr += S->m;
+    max_m = std::max(max_m, S->m);
+    fp.push_back(&S->fused32);
+    ap.push_back(&S->apply32);
+    mp.push_back(&S->mv_sol);
+    const long long n = S->N;
+    auto add_in = [&](const double *src, float *dst, long long cols) {
+      if (cols <= 0) return;
+      cin.push_back({src, n, dst, n, n, cols});
+      t_in = std::max(t_in, ew2d_tiles(n, cols));
+    };
+    add_in(S->D.p, S->D32.p, S->nmax);
+    add_in(S->B.p, S->X32.p, S->m);
+    add_in(S->U.p, S->X32.p + (size_t)n * S->m, S->vc);
+    add_in(S->V.p, S->V32.p, S->vc);
+    cres.push_back({S->R64.p, n, S->Y32.p, n, n, S->m});
+    t_res = std::max(t_res, ew2d_tiles(n, S->m));
+    cx0.push_back({S->X32.p, n, S->Xsol.p, n, n, S->m});
+    addy.push_back({S->Y32.p, n, S->Xsol.p, n, n, S->m});
+    t_x0 = std::max(t_x0, ew2d_tiles(n, S->m));
+  }
+  rr.ensure(std::max(n_rr, 1));
+  for (size_t k = 0; k < sys.size(); ++k) {
+    System *S = sys[k];
+    RatioTask t{};
+    t.r = S->R64.p;
+    t.ldr = S->N;
+    t.b = S->B.p;
+    t.ldb = S->N;
+    t.rows = S->N;
+    t.out = rr.p + rr_off[k];
+    t.cols = S->m;
+    rt.push_back(t);
+  }
+  merge_paths<float, float>(fp, info_off, fused32);
+  merge_paths<float, float>(ap, info_off, apply32);
+  merge_matvecs(mp, mv);
+  cv_in.upload(cin);
+  cv_res.upload(cres);
+  cv_x0.upload(cx0);
+  add_y.upload(addy);
+  ratios.upload(rt);
+  info.ensure(n_info);
+  HODLR_CUDA_TRY(cudaMemset(info.p, 0, sizeof(int) * n_info));
+  g_factor.reset();
+  g_sweep.reset();
+}
+
+void Batch::residuals(cudaStream_t s) {
+  matvec_launches(prof, mv, -1.0, 1.0, s);
+  launch_colratio_batched(ratios.p, (int)sys.size(), max_m, s);
+}
+
+void Batch::run_factor(cudaStream_t s) {
+  {
+    PhaseScope ps(prof, PH_CONVERT, s);
+    launch_ew2d_batched<double, float>(cv_in.p, (int)cv_in.h.size(), t_in, false, s);
+  }
+  run_path(prof, fused32, 0, info.p, s);
+  launch_ew2d_batched<float, double>(cv_x0.p, (int)cv_x0.h.size(), t_x0, false, s);
+  residuals(s);
+}
+
+void Batch::run_sweep(cudaStream_t s) {
+  launch_ew2d_batched<double, float>(cv_res.p, (int)cv_res.h.size(), t_res, false, s);
+  run_path(prof, apply32, 0, nullptr, s);
+  launch_ew2d_batched<float, double>(add_y.p, (int)add_y.h.size(), t_x0, true, s);
+  residuals(s);
+}
+
+int Batch::check_info(cudaStream_t s, int *failed) {
+  std::vector<int> h(n_info);
+  HODLR_CUDA_TRY(cudaMemcpyAsync(h.data(), info.p, sizeof(int) * n_info, cudaMemcpyDeviceToHost, s));
+  HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (failed) *failed = -1;
+  for (size_t k = 0; k < sys.size(); ++k) {
+    const int nl = (int)sys[k]->tree.leaves.size();
+    for (int i = 0; i < sys[k]->n_info; ++i) {
+      const int v = h[info_off[k] + i];
+      if (v == 0) continue;
+      if (failed) *failed = (int)k;
+      return i < nl ? v : 100000 + v;
+    }
+  }
+  return 0;
+}
+
+double Batch::relres_read(cudaStream_t s, std::vector<double> *per_system) {
+  const int n_rr = rr_off.back() + sys.back()->m;
+  std::vector<double> h(n_rr);
+  HODLR_CUDA_TRY(cudaMemcpyAsync(h.data(), rr.p, sizeof(double) * n_rr, cudaMemcpyDeviceToHost, s));
+  HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+  double mx = 0.0;
+  if (per_system) per_system->assign(sys.size(), 0.0);
+  for (size_t k = 0; k < sys.size(); ++k) {
+    double mk = 0.0;
+    for (int c = 0; c < sys[k]->m; ++c) {
+      const double v = h[rr_off[k] + c];
+      mk = std::max(mk, std::isnan(v) ? INFINITY : v);
+    }
+    if (per_system) (*per_system)[k] = mk;
+    mx = std::max(mx, mk);
+  }
   return mx;
 }
 

@@ -18,6 +18,7 @@ template <typename T>
 struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
+  std::vector<T> h;  // host copy of the last upload (launch descriptors, for merging plans)
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
@@ -40,6 +41,7 @@ struct DevBuf {
     n = count;
   }
   void upload(const std::vector<T> &v) {
+    h = v;
     ensure(v.size());
     if (!v.empty()) HODLR_CUDA_TRY(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
   }
@@ -166,10 +168,47 @@ struct GraphSeg {
   GraphSeg() = default;
   GraphSeg(const GraphSeg &) = delete;
   GraphSeg &operator=(const GraphSeg &) = delete;
-  ~GraphSeg() {
+  ~GraphSeg() { reset(); }
+  void reset() {
     if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    kernels = 0;
   }
 };
+
+// Runs `fn` (stream work on s) through the graph cache `g`: captured on the
+// first call, replayed afterwards; eager when `eager` is set or on the legacy
+// default stream (which cannot be captured).
+template <typename F>
+void run_graph(GraphSeg &g, bool eager, cudaStream_t s, F &&fn) {
+  if (eager || s == nullptr) {
+    fn();
+    return;
+  }
+  if (!g.exec) {
+    const long long before = launch_total();
+    cudaGraph_t graph = nullptr;
+    HODLR_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      fn();
+    } catch (...) {
+      cudaStreamEndCapture(s, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    HODLR_CUDA_TRY(cudaStreamEndCapture(s, &graph));
+    cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      g.exec = nullptr;
+      throw CudaError{e};
+    }
+    g.kernels = launch_total() - before;
+    add_launches(-g.kernels);  // counted when replayed
+  }
+  HODLR_CUDA_TRY(cudaGraphLaunch(g.exec, s));
+  add_launches(g.kernels);
+}
 
 struct System {
   Tree tree;
@@ -195,6 +234,7 @@ struct System {
   int factored = -1;  // HODLR_PREC_* of the current factorization, -1 none
   int factored_form = 0;
   int red_chunk = 512;
+  int nb32 = 0;  // forced FP32 leaf panel width (0: by the largest leaf); batches align it
   int bc_chunk = 512;
   int n_info = 0;
   Profiler prof;
@@ -208,44 +248,59 @@ struct System {
   void run_fused64(int form, cudaStream_t s);     // X64 = [B|U], DLU64 = D, walk
   void run_apply64(cudaStream_t s);               // Y64 <- A^{-1} Y64 with fused64 factors
   void run_factor32(cudaStream_t s);              // X32 = f32([B|U]), D32 = f32(D), walk
+  void convert32(cudaStream_t s);                 // the FP64 -> FP32 copies of run_factor32
   void run_apply32(cudaStream_t s);               // Y32 <- A^{-1} Y32
   void run_matvec(const MatvecPlan &p, double alpha, double beta, cudaStream_t s);
   int check_info(cudaStream_t s);                 // sync + first nonzero INFO
   double relres(cudaStream_t s);                  // of Xsol against B (sync)
   void relres_enqueue(cudaStream_t s);            // matvec + column ratios into relres_dev
   double relres_read(cudaStream_t s);             // sync + max of relres_dev
-  // Runs `fn` (stream work on s) through the graph cache `g`: captured on the
-  // first call, replayed afterwards; eager when graphs are off, while
-  // profiling, or on the legacy default stream (which cannot be captured).
   template <typename F>
   void run_graph(GraphSeg &g, cudaStream_t s, F &&fn) {
-    if (!use_graphs || prof.on || s == nullptr) {
-      fn();
-      return;
-    }
-    if (!g.exec) {
-      const long long before = launch_total();
-      cudaGraph_t graph = nullptr;
-      HODLR_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      try {
-        fn();
-      } catch (...) {
-        cudaStreamEndCapture(s, &graph);
-        if (graph) cudaGraphDestroy(graph);
-        throw;
-      }
-      HODLR_CUDA_TRY(cudaStreamEndCapture(s, &graph));
-      cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess) {
-        g.exec = nullptr;
-        throw CudaError{e};
-      }
-      g.kernels = launch_total() - before;
-      add_launches(-g.kernels);  // counted when replayed
-    }
-    HODLR_CUDA_TRY(cudaGraphLaunch(g.exec, s));
-    add_launches(g.kernels);
+    ::hodlr::run_graph(g, !use_graphs || prof.on, s, fn);
+  }
+  void reset_graphs() {
+    g_factor32.reset(); g_sweep32.reset(); g_factor64.reset(); g_sweep64.reset();
+    g_fused64[0].reset(); g_fused64[1].reset();
+  }
+};
+
+// Many independent systems of uneven size, rank and right-hand-side count
+// solved together: their level schedules are merged step by step (every
+// leaf panel of every system in one launch, then each system's deepest
+// remaining level in one launch per phase, ...), so the batch costs one
+// launch per tree level and phase rather than one per system.  Mixed
+// precision with FP64 refinement; every system keeps its own buffers and
+// factors, and the merged plans only hold launch descriptors that point into
+// them.  The systems must outlive the batch and keep their sizes.
+struct Batch {
+  std::vector<System *> sys;
+  PathPlan<float, float> fused32, apply32;
+  MatvecPlan mv;
+  DevBuf<Ew2DTask<double, float>> cv_in, cv_res;  // D, B, U, V -> FP32; R64 -> Y32
+  DevBuf<Ew2DTask<float, double>> cv_x0, add_y;   // X32 -> Xsol; Xsol += Y32
+  long long t_in = 0, t_res = 0, t_x0 = 0;        // largest tile count of each
+  DevBuf<RatioTask> ratios;
+  int max_m = 0;
+  DevBuf<double> rr;            // column residual ratios, system k at rr_off[k]
+  std::vector<int> rr_off;
+  DevBuf<int> info;             // all systems' INFO slots, system k at info_off[k]
+  std::vector<int> info_off;
+  int n_info = 0, nb = 0;
+  bool use_graphs = true;
+  GraphSeg g_factor, g_sweep;
+  Profiler prof;
+  void build(const std::vector<System *> &systems);
+  void run_factor(cudaStream_t s);   // conversions, merged walk, x0, residuals
+  void run_sweep(cudaStream_t s);    // one refinement sweep of every system, residuals
+  void residuals(cudaStream_t s);    // merged matvec R = B - A Xsol + column ratios
+  // sync; the first nonzero INFO (leaf code, or 100000 + node code) and its system
+  int check_info(cudaStream_t s, int *failed);
+  // sync; the largest ratio, and each system's largest in per_system
+  double relres_read(cudaStream_t s, std::vector<double> *per_system);
+  template <typename F>
+  void run_graph(GraphSeg &g, cudaStream_t s, F &&fn) {
+    ::hodlr::run_graph(g, !use_graphs || prof.on, s, fn);
   }
 };
 

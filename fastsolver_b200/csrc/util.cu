@@ -61,6 +61,55 @@ __global__ void colratio_kernel(const double *__restrict__ r, long long ldr,
   }
 }
 
+// Batched element-wise pass: blockIdx.y picks the task, blockIdx.x strides
+// over its (column, 1024-row tile) pairs; each thread moves 4 rows of a tile,
+// consecutive threads on consecutive rows (coalesced on both sides).
+template <typename TS, typename TD, bool ADD>
+__global__ void ew2d_batched_kernel(const Ew2DTask<TS, TD> *__restrict__ tasks) {
+  const Ew2DTask<TS, TD> tk = tasks[blockIdx.y];
+  const long long rtiles = cdiv<long long>(tk.rows, kEwTileRows);
+  const long long ntiles = rtiles * tk.cols;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const long long j = t / rtiles;
+    const long long i0 = (t - j * rtiles) * kEwTileRows;
+    const TS *src = tk.src + j * tk.lds;
+    TD *dst = tk.dst + j * tk.ldd;
+#pragma unroll
+    for (int q = 0; q < kEwTileRows / kThreads; ++q) {
+      const long long i = i0 + q * kThreads + threadIdx.x;
+      if (i < tk.rows) {
+        if (ADD) dst[i] += TD(src[i]);
+        else dst[i] = TD(src[i]);
+      }
+    }
+  }
+}
+
+// Batched colratio_kernel: blockIdx.y picks the system, blockIdx.x the column.
+__global__ void colratio_batched_kernel(const RatioTask *__restrict__ tasks) {
+  __shared__ double sr[32], sb[32];
+  const RatioTask tk = tasks[blockIdx.y];
+  const int c = blockIdx.x;
+  if (c >= tk.cols) return;
+  double ar = 0.0, ab = 0.0;
+  for (long long i = threadIdx.x; i < tk.rows; i += blockDim.x) {
+    const double x = tk.r[i + c * tk.ldr], y = tk.b[i + c * tk.ldb];
+    ar += x * x;
+    ab += y * y;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    ar += __shfl_down_sync(0xffffffffu, ar, off);
+    ab += __shfl_down_sync(0xffffffffu, ab, off);
+  }
+  if ((threadIdx.x & 31) == 0) { sr[threadIdx.x >> 5] = ar; sb[threadIdx.x >> 5] = ab; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tr = 0.0, tb = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tr += sr[w]; tb += sb[w]; }
+    tk.out[c] = tb > 0.0 ? sqrt(tr) / sqrt(tb) : sqrt(tr);
+  }
+}
+
 // dst[t][e] = sum_q src[t] + q * stride, fixed order (deterministic)
 template <typename T>
 __global__ void sum_slots_kernel(const SumTask<T> *__restrict__ tasks) {
@@ -275,12 +324,38 @@ void launch_colratio(const double *r, long long ldr, const double *b, long long 
   HODLR_LAUNCH_CHECK();
 }
 
+template <typename TS, typename TD>
+void launch_ew2d_batched(const Ew2DTask<TS, TD> *tasks, int ntasks, long long max_tiles,
+                         bool add, cudaStream_t s) {
+  if (ntasks <= 0 || max_tiles <= 0) return;
+  // about 8 resident CTAs of 256 threads per SM over all tasks
+  const long long want = std::max<long long>(1, 148LL * 8 / ntasks);
+  dim3 grid((unsigned)std::min<long long>(max_tiles, std::max<long long>(want, 4)), ntasks);
+  if (add) ew2d_batched_kernel<TS, TD, true><<<grid, kThreads, 0, s>>>(tasks);
+  else ew2d_batched_kernel<TS, TD, false><<<grid, kThreads, 0, s>>>(tasks);
+  HODLR_LAUNCH_CHECK();
+}
+template void launch_ew2d_batched<double, float>(const Ew2DTask<double, float> *, int, long long,
+                                                 bool, cudaStream_t);
+template void launch_ew2d_batched<float, double>(const Ew2DTask<float, double> *, int, long long,
+                                                 bool, cudaStream_t);
+
+void launch_colratio_batched(const RatioTask *tasks, int ntasks, int max_cols, cudaStream_t s) {
+  if (ntasks <= 0 || max_cols <= 0) return;
+  colratio_batched_kernel<<<dim3(max_cols, ntasks), 1024, 0, s>>>(tasks);
+  HODLR_LAUNCH_CHECK();
+}
+
 template <typename T>
 void launch_sum_slots(const SumTask<T> *tasks, int ntasks, long long max_len, cudaStream_t s) {
   if (ntasks <= 0 || max_len <= 0) return;
-  dim3 grid((unsigned)std::min<long long>(cdiv<long long>(max_len, kThreads), 4096), ntasks);
-  sum_slots_kernel<T><<<grid, kThreads, 0, s>>>(tasks);
-  HODLR_LAUNCH_CHECK();
+  // grid.y is at most 65535: merged batches can hold more tasks than that
+  for (int t0 = 0; t0 < ntasks; t0 += 65535) {
+    dim3 grid((unsigned)std::min<long long>(cdiv<long long>(max_len, kThreads), 4096),
+              std::min(65535, ntasks - t0));
+    sum_slots_kernel<T><<<grid, kThreads, 0, s>>>(tasks + t0);
+    HODLR_LAUNCH_CHECK();
+  }
 }
 template void launch_sum_slots<double>(const SumTask<double> *, int, long long, cudaStream_t);
 template void launch_sum_slots<float>(const SumTask<float> *, int, long long, cudaStream_t);

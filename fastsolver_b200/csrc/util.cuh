@@ -55,4 +55,39 @@ void launch_gauss_fill_batched(const FillTask *tasks, int ntasks, long long max_
                                unsigned long long seed, cudaStream_t s);
 void launch_scale_batched(const FillTask *tasks, int ntasks, long long max_elems, cudaStream_t s);
 
+// One block of a batched element-wise pass over column-major matrices:
+// dst(i, j) = TD(src(i, j)), or dst(i, j) += TD(src(i, j)).
+template <typename TS, typename TD>
+struct Ew2DTask {
+  const TS *src;
+  long long lds;
+  TD *dst;
+  long long ldd;
+  long long rows;
+  long long cols;
+};
+template <typename TS, typename TD>
+void launch_ew2d_batched(const Ew2DTask<TS, TD> *tasks, int ntasks, long long max_tiles,
+                         bool add, cudaStream_t s);
+// Row tiles of the batched pass (launch_ew2d_batched's max_tiles is the
+// largest of these over the tasks).
+constexpr int kEwTileRows = 1024;
+inline long long ew2d_tiles(long long rows, long long cols) {
+  return cdiv<long long>(rows, kEwTileRows) * cols;
+}
+
+// Per-column residual ratios of one system of a batch:
+// out[c] = ||r(:, c)|| / ||b(:, c)||, c < cols.
+struct RatioTask {
+  const double *r;
+  long long ldr;
+  const double *b;
+  long long ldb;
+  long long rows;
+  double *out;
+  int cols;
+  int pad;
+};
+void launch_colratio_batched(const RatioTask *tasks, int ntasks, int max_cols, cudaStream_t s);
+
 }  // namespace hodlr

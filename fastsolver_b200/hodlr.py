@@ -23,7 +23,7 @@ import numpy as np
 from . import _lib
 from ._lib import PREC_FP64, PREC_MIXED, NODE_FIELDS, call, check, lib
 
-__all__ = ["HodlrMatrix", "FastSolver", "build_tree", "leaf_solve", "gemm_reduce",
+__all__ = ["HodlrMatrix", "FastSolver", "SystemBatch", "build_tree", "leaf_solve", "gemm_reduce",
            "gemm_broadcast", "node_lu_solve", "node_schur2_solve", "PREC_FP64", "PREC_MIXED"]
 
 
@@ -275,6 +275,54 @@ class FastSolver:
         if check_conv or st != _lib.ERR_NOCONV:
             check("hodlr_solve_refined", st)
         return it.value, rr.value
+
+
+class SystemBatch:
+    """Independent HODLR systems of uneven size, rank, leaf size and RHS count
+    solved together (one merged launch per tree level and phase).  The
+    matrices keep their own data: load matrices and RHS into them as usual,
+    call solve_refined, then read each matrix's solution().  The matrices must
+    stay open while the batch exists."""
+
+    def __init__(self, matrices):
+        self.matrices = list(matrices)
+        arr = (ctypes.c_void_p * len(self.matrices))(*[m.handle.value for m in self.matrices])
+        h = ctypes.c_void_p()
+        call("hodlr_batch_create", ctypes.byref(h), arr, len(self.matrices))
+        self._h = h
+
+    def solve_refined(self, tol: float = 1e-12, maxiter: int = 10, stream=None,
+                      check_conv=True):
+        """Returns (sweeps, per-system relative residuals)."""
+        it, mx, failed = ctypes.c_int(), ctypes.c_double(), ctypes.c_int(-1)
+        rr = (ctypes.c_double * len(self.matrices))()
+        st = lib.hodlr_batch_solve_refined(self._h, float(tol), int(maxiter), ctypes.byref(it),
+                                           ctypes.byref(mx), rr, ctypes.byref(failed),
+                                           _stream_ptr(stream))
+        self.failed = failed.value
+        if check_conv or st != _lib.ERR_NOCONV:
+            check("hodlr_batch_solve_refined", st)
+        return it.value, list(rr)
+
+    def set_profiling(self, on: bool):
+        call("hodlr_batch_set_profiling", self._h, int(bool(on)))
+
+    def phase_times(self, reset: bool = True) -> dict:
+        ms = (ctypes.c_double * len(_lib.PHASES))()
+        ln = (ctypes.c_longlong * len(_lib.PHASES))()
+        call("hodlr_batch_phase_times", self._h, ms, ln, int(reset))
+        return {k: (ms[i], int(ln[i])) for i, k in enumerate(_lib.PHASES)}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib.hodlr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

@@ -248,6 +248,39 @@ int hodlr_set_profiling(hodlr_system sys, int on);
 int hodlr_phase_times(hodlr_system sys, double *ms, long long *launches,
                       int reset);
 
+/* ---- Batches of independent systems (no reference counterpart: the
+ * reference solves one system per Legion run).  A batch merges the level
+ * schedules of `count` systems of any size, rank, leaf size and RHS count
+ * (created by hodlr_create, matrices and RHS loaded): every leaf panel of
+ * every system runs in one launch, then level j (deepest first) of every
+ * system in one launch per phase, and the residual matvecs of all systems
+ * in one launch.  1 <= count <= 16384.  The systems must outlive the batch
+ * and must not be destroyed, re-created or put into another batch while it
+ * exists; loading new matrices or RHS into them is fine (a solve reads their
+ * buffers). */
+typedef struct hodlr_batch_s *hodlr_batch;
+int hodlr_batch_create(hodlr_batch *out, const hodlr_system *systems, int count);
+int hodlr_batch_destroy(hodlr_batch batch);
+
+/* Mixed-precision solve of every system of the batch with FP64 iterative
+ * refinement until each system's max_j ||b_j - A x_j|| / ||b_j|| <= tol (or
+ * maxiter sweeps, all systems sweeping together).  iters, relres_max (host
+ * scalars), relres (host array of `count`, each system's residual) and
+ * failed (the system whose factorization reported a nonzero INFO, -1 if
+ * none) may be NULL.  Returns 0, the failing system's INFO (leaf INFO, or
+ * 100000 + node INFO, as hodlr_solve_fused), or HODLR_ERR_NOCONV.  On a
+ * non-default stream the factor pass and the sweep are captured as CUDA
+ * graphs on first use and replayed afterwards.  Each system's solution is
+ * read with hodlr_get_solution; each system is left factored (hodlr_solve
+ * applies the same factors to a new RHS). */
+int hodlr_batch_solve_refined(hodlr_batch batch, double tol, int maxiter, int *iters,
+                              double *relres_max, double *relres, int *failed,
+                              hodlr_stream_t stream);
+
+/* Per-phase device time of the batch's merged launches (as hodlr_phase_times). */
+int hodlr_batch_set_profiling(hodlr_batch batch, int on);
+int hodlr_batch_phase_times(hodlr_batch batch, double *ms, long long *launches, int reset);
+
 /* Number of kernels this library launched on this thread since the last
  * reset (every launch from a hodlr_* call is counted). */
 long long hodlr_launch_count(void);

@@ -56,6 +56,15 @@ def test_argument_errors_are_reported_before_device_use(fs):
     assert lib.hodlr_gemm_broadcast(-1.0, 1.0, 4, 2, 2, 8, 4, 0, 8, 2, 1, None) == -11
     assert lib.hodlr_solve(None, None) == -1
     assert lib.hodlr_status_string(-1003) == b"refinement did not reach the tolerance"
+    h = ctypes.c_void_p()
+    two = (ctypes.c_void_p * 2)(None, None)
+    assert lib.hodlr_batch_create(None, two, 2) == -1
+    assert lib.hodlr_batch_create(ctypes.byref(h), None, 2) == -2
+    assert lib.hodlr_batch_create(ctypes.byref(h), two, 2) == -2   # null system handle
+    assert lib.hodlr_batch_create(ctypes.byref(h), two, 0) == -3
+    assert h.value is None
+    assert lib.hodlr_batch_solve_refined(None, 1e-12, 10, None, None, None, None, None) == -1
+    assert lib.hodlr_batch_destroy(None) == -1
 
 
 @pytest.mark.skipif(cuda_available(), reason="checks the no-device status")
