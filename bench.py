@@ -45,6 +45,11 @@ CONFIGS = {
     "n1048576": dict(N=1048576, leaf=512, rank=100, nrhs=32),
 }
 METRIC = "solves/s at N=2^18,r=64: mixed+batched vs plain FP64 GPU @relres<=1e-12"
+# batched workload: 64 independent systems, N log-uniform in [8192, 131072],
+# leaf size from {256, 512, 1024}, rank uniform in [16, 96], 1..32 RHS
+BATCH = dict(count=64, n_lo=8192, n_hi=131072, leaves=(256, 512, 1024), rank=(16, 96),
+             nrhs=(1, 32))
+BATCH_METRIC = "systems solved/s: 64 uneven HODLR systems, batched mixed @relres<=1e-12"
 TOL = 1e-12
 
 
@@ -232,6 +237,127 @@ def make_system(fs, cfg, seed):
     return h
 
 
+def batch_systems(seed: int, count: int = BATCH["count"]):
+    """The batched workload's seeded draw of system shapes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        N = int(round(np.exp(rng.uniform(np.log(BATCH["n_lo"]), np.log(BATCH["n_hi"])))))
+        leaf = int(rng.choice(BATCH["leaves"]))
+        rank = int(rng.integers(BATCH["rank"][0], BATCH["rank"][1] + 1))
+        nrhs = int(rng.integers(BATCH["nrhs"][0], BATCH["nrhs"][1] + 1))
+        out.append(dict(N=N, leaf=leaf, rank=rank, nrhs=nrhs))
+    return out
+
+
+def run_batch(args):
+    """Batched workload: every step solves all systems of the draw in one
+    merged schedule (SystemBatch, mixed precision + FP64 refinement to
+    relres <= 1e-12).  Beside it: the same systems solved one after another
+    with the single-system mixed solve, and with the plain FP64 path."""
+    import torch
+    import fastsolver_b200 as fs
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    cfgs = batch_systems(args.seed)
+    hs = [make_system(fs, c, args.seed + 7919 * rank + i) for i, c in enumerate(cfgs)]
+    batch = fs.SystemBatch(hs)
+    solver = fs.FastSolver()
+
+    def batch_step():
+        return batch.solve_refined(tol=TOL, maxiter=10, stream=stream)
+
+    if args.profile_one:
+        for _ in range(2):
+            batch_step()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        batch_step()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(f"profiled one batched solve of {len(hs)} systems", flush=True)
+        return
+
+    def timed(fn, steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        e0.record(stream)
+        out = [fn() for _ in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return rank_max(e0.elapsed_time(e1) / steps, dist, "cuda"), out
+
+    for _ in range(args.warmup):
+        batch_step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    fs.reset_launch_count()
+    ms_batch, outs = timed(batch_step, args.steps)
+    launches = fs.launch_count()
+    clk = clocks.stop()
+    sweeps = [o[0] for o in outs]
+    rr_max = max(max(o[1]) for o in outs)
+
+    def seq_mixed():
+        return [solver.solve_refined(h, fs.PREC_MIXED, tol=TOL, maxiter=10, stream=stream)
+                for h in hs]
+
+    def seq_fp64():
+        for h in hs:
+            solver.bfs_solve(h, sync=False, stream=stream)
+
+    for _ in range(2):
+        seq_mixed()
+    ms_seq, _ = timed(seq_mixed, max(1, args.steps // 2))
+    for _ in range(2):
+        seq_fp64()
+    ms_fp64, _ = timed(seq_fp64, max(1, args.steps // 2))
+    rr_fp64 = max(h.relres(stream=stream) for h in hs)
+
+    batch.set_profiling(True)
+    batch_step()
+    ph = batch.phase_times(reset=True)
+    batch.set_profiling(False)
+    if rank == 0:
+        n = len(hs)
+        line = {
+            "metric": BATCH_METRIC, "value": ws * n * 1e3 / ms_batch, "unit": "systems/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64",
+            "data": "synthetic (seeded Gaussian HODLR systems generated on the device)",
+            "config": {"workload": f"{n} uneven HODLR systems, batched mixed+refine to "
+                                   f"relres<=1e-12", **BATCH,
+                       "unknowns": int(sum(c["N"] for c in cfgs)), "seed": args.seed,
+                       "parallelism": f"replicas x{ws}",
+                       "l2": "inputs tens of GB > L2"},
+            "relres_max": rr_max, "refine_sweeps": sweeps,
+            "sequential_mixed": {"value": ws * n * 1e3 / ms_seq, "unit": "systems/s",
+                                 "ms_per_step": ms_seq},
+            "sequential_fp64": {"value": ws * n * 1e3 / ms_fp64, "unit": "systems/s",
+                                "ms_per_step": ms_fp64, "relres": rr_fp64},
+            "batched_over_sequential_mixed": ms_seq / ms_batch,
+            "batched_over_sequential_fp64": ms_fp64 / ms_batch,
+            "phases_ms": {k: round(v[0], 4) for k, v in ph.items()},
+            "gpu_launches": int(launches), "clocks": clk,
+            "e2e": None, "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 # ---------------------------------------------------------------------------
 # reference arm: the CPU oracle (restated reference path) on the host cores
 # ---------------------------------------------------------------------------
@@ -279,16 +405,22 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="n262144", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="n262144", choices=sorted(CONFIGS) + ["batch64"])
     ap.add_argument("--seed", type=int, default=1245667)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-solves", type=int, default=2)
-    ap.add_argument("--profile-one", choices=["mixed", "fp64"], default=None,
+    ap.add_argument("--profile-one", choices=["mixed", "fp64", "batch"], default=None,
                     help="warm up, then run one solve between cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no bench line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.config == "batch64":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the batched workload has "
+                              "no reference counterpart (one system per reference run)"}))
+            return
+        return run_batch(args)
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, cfg)

@@ -332,7 +332,8 @@ constexpr int kDmmaKT = 8;              // NN: K per stage
 constexpr int kDmmaStages = 3;
 constexpr int kDmmaAP = kDmmaRows + 8;  // padded k-row stride (doubles)
 
-// NN: C (M x N <= 16) = beta Cin + alpha sum_s A_s B_s, A_s column-major
+// NN: C (M x N) = beta Cin + alpha sum_s A_s B_s, A_s column-major; one CTA
+// per (item, 512-row block, block of 8 NT8 columns)
 template <int NT8>
 __global__ void __launch_bounds__(kSkThreads, 2)
     skinny_nn_dmma_kernel(const GemmItem<double, double> *__restrict__ items,
@@ -343,10 +344,11 @@ __global__ void __launch_bounds__(kSkThreads, 2)
   double *Bs = As + (size_t)kDmmaStages * KT * AP;         // [stage][KT][NCS]
   const GemmItem<double, double> it = items[blockIdx.x];
   const int row0 = blockIdx.y * ROWS;
-  if (row0 >= it.M) return;
+  const int n0 = blockIdx.z * NCS;  // column block of this CTA
+  if (row0 >= it.M || n0 >= it.N) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int N = it.N;
+  const int N = it.N - n0;  // columns left from n0
 
   auto load = [&](const TileIter<double> &p, int st) {
     if (p.valid) {
@@ -374,7 +376,8 @@ __global__ void __launch_bounds__(kSkThreads, 2)
       for (int e = tid; e < KT * NCS; e += kSkThreads) {
         const int k = e % KT, n = e / KT;
         const bool ok = (p.k0 + k < sg.K) && n < N;
-        cpa(b + k * NCS + n, ok ? sg.B + (p.k0 + k) + (long long)n * sg.ldb : sg.B, 8, ok);
+        cpa(b + k * NCS + n, ok ? sg.B + (p.k0 + k) + (long long)(n0 + n) * sg.ldb : sg.B, 8,
+            ok);
       }
     }
     cpa_commit();
@@ -430,11 +433,12 @@ __global__ void __launch_bounds__(kSkThreads, 2)
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         const int row = row0 + wrow + mt * 16 + g + (v >> 1) * 8;
-        const int col = nt * 8 + 2 * t + (v & 1);
-        if (row < it.M && col < N) {
+        const int c = nt * 8 + 2 * t + (v & 1);
+        if (row < it.M && c < N) {
+          const long long col = n0 + c;
           double val = alpha * acc[mt][nt][v];
-          if (it.Cin) val += beta * it.Cin[row + (long long)col * it.ldcin];
-          it.C[row + (long long)col * it.ldc] = val;
+          if (it.Cin) val += beta * it.Cin[row + col * it.ldcin];
+          it.C[row + col * it.ldc] = val;
         }
       }
 }
@@ -535,28 +539,27 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
                    int max_n, bool trans, T alpha, T beta, cudaStream_t s) {
   if (nitems <= 0 || max_m <= 0 || max_n <= 0) return;
   if constexpr (sizeof(T) == 8) {
-    if (max_n <= 16) {
-      if (trans) {
-        const size_t smem = (size_t)kSkStages * (64 + 16) * kDmmaLDK * sizeof(double);
-        HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_tn_dmma_kernel,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        dim3 grid(nitems, cdiv(max_m, 64), cdiv(max_n, 16));
-        skinny_tn_dmma_kernel<<<grid, kTNThreads, smem, s>>>(items, segs, alpha, beta);
-      } else {
-        dim3 grid(nitems, cdiv(max_m, kDmmaRows));
-        auto go = [&](auto kern, int ncs) {
-          const size_t smem =
-              (size_t)kDmmaStages * kDmmaKT * (kDmmaAP + ncs) * sizeof(double);
-          HODLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)smem));
-          kern<<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);
-        };
-        if (max_n <= 8) go(skinny_nn_dmma_kernel<1>, 8);
-        else go(skinny_nn_dmma_kernel<2>, 16);
-      }
-      HODLR_LAUNCH_CHECK();
-      return;
+    // FP64 products run on the FP64 tensor pipe (DMMA)
+    if (trans) {
+      const size_t smem = (size_t)kSkStages * (64 + 16) * kDmmaLDK * sizeof(double);
+      HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_tn_dmma_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      dim3 grid(nitems, cdiv(max_m, 64), cdiv(max_n, 16));
+      skinny_tn_dmma_kernel<<<grid, kTNThreads, smem, s>>>(items, segs, alpha, beta);
+    } else {
+      // 8 columns per CTA when every item has at most 8, else 16-column blocks
+      dim3 grid(nitems, cdiv(max_m, kDmmaRows), max_n <= 8 ? 1 : cdiv(max_n, 16));
+      auto go = [&](auto kern, int ncs) {
+        const size_t smem = (size_t)kDmmaStages * kDmmaKT * (kDmmaAP + ncs) * sizeof(double);
+        HODLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+        kern<<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);
+      };
+      if (max_n <= 8) go(skinny_nn_dmma_kernel<1>, 8);
+      else go(skinny_nn_dmma_kernel<2>, 16);
     }
+    HODLR_LAUNCH_CHECK();
+    return;
   }
   if (trans) {
     constexpr int TM = 64, TN = 16, KC = 32, LDK = KC + 16 / sizeof(T);

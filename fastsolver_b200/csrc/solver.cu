@@ -1007,54 +1007,55 @@ double System::relres_read(cudaStream_t s) {
 void Batch::build(const std::vector<System *> &systems) {
   if (systems.empty()) throw CudaError{cudaErrorInvalidValue};
   sys = systems;
-  // one FP32 leaf panel width for all: the merged panel launches share it
-  int gmax = 0;
-  for (System *S : sys) gmax = std::max(gmax, S->nmax);
-  nb = leaf_nb<float>(gmax);
-  for (System *S : sys) {
-    if (S->fused32.built && S->fused32.leaf.nb != nb) {
-      S->fused32.built = false;  // rebuild the plans with the common width
-      S->reset_graphs();
-    }
-    S->nb32 = nb;
+  groups.clear();
+  for (size_t k = 0; k < sys.size(); ++k) {
+    System *S = sys[k];
     S->ensure_mixed();
+    const int nbk = S->fused32.leaf.nb;
+    const bool wide = S->m > 16;
+    Group *g = nullptr;
+    for (auto &q : groups)
+      if (q->nb == nbk && q->wide == wide) g = q.get();
+    if (!g) {
+      groups.push_back(std::make_unique<Group>());
+      g = groups.back().get();
+      g->nb = nbk;
+      g->wide = wide;
+    }
+    g->members.push_back((int)k);
   }
   info_off.clear();
   rr_off.clear();
   n_info = 0;
   int n_rr = 0;
   max_m = 0;
-  std::vector<const PathPlan<float, float> *> fp, ap;
   std::vector<const MatvecPlan *> mp;
   std::vector<Ew2DTask<double, float>> cin, cres;
   std::vector<Ew2DTask<float, double>> cx0, addy;
   std::vector<RatioTask> rt;
-  t_in = t_res = t_x0 = 0;
   for (System *S : sys) {
     info_off.push_back(n_info);
     n_info += S->n_info;
     rr_off.push_back(n_rr);
     n_rr += S->m;
     max_m = std::max(max_m, S->m);
-    fp.push_back(&S->fused32);
-    ap.push_back(&S->apply32);
     mp.push_back(&S->mv_sol);
     const long long n = S->N;
     auto add_in = [&](const double *src, float *dst, long long cols) {
-      if (cols <= 0) return;
-      cin.push_back({src, n, dst, n, n, cols});
-      t_in = std::max(t_in, ew2d_tiles(n, cols));
+      if (cols > 0) cin.push_back({src, n, dst, n, n, cols, 0});
     };
     add_in(S->D.p, S->D32.p, S->nmax);
     add_in(S->B.p, S->X32.p, S->m);
     add_in(S->U.p, S->X32.p + (size_t)n * S->m, S->vc);
     add_in(S->V.p, S->V32.p, S->vc);
-    cres.push_back({S->R64.p, n, S->Y32.p, n, n, S->m});
-    t_res = std::max(t_res, ew2d_tiles(n, S->m));
-    cx0.push_back({S->X32.p, n, S->Xsol.p, n, n, S->m});
-    addy.push_back({S->Y32.p, n, S->Xsol.p, n, n, S->m});
-    t_x0 = std::max(t_x0, ew2d_tiles(n, S->m));
+    cres.push_back({S->R64.p, n, S->Y32.p, n, n, S->m, 0});
+    cx0.push_back({S->X32.p, n, S->Xsol.p, n, n, S->m, 0});
+    addy.push_back({S->Y32.p, n, S->Xsol.p, n, n, S->m, 0});
   }
+  t_in = ew2d_prefix(cin);
+  t_res = ew2d_prefix(cres);
+  t_x0 = ew2d_prefix(cx0);
+  ew2d_prefix(addy);
   rr.ensure(std::max(n_rr, 1));
   for (size_t k = 0; k < sys.size(); ++k) {
     System *S = sys[k];
@@ -1068,8 +1069,17 @@ void Batch::build(const std::vector<System *> &systems) {
     t.cols = S->m;
     rt.push_back(t);
   }
-  merge_paths<float, float>(fp, info_off, fused32);
-  merge_paths<float, float>(ap, info_off, apply32);
+  for (auto &g : groups) {
+    std::vector<const PathPlan<float, float> *> fp, ap;
+    std::vector<int> off;
+    for (int k : g->members) {
+      fp.push_back(&sys[k]->fused32);
+      ap.push_back(&sys[k]->apply32);
+      off.push_back(info_off[k]);
+    }
+    merge_paths<float, float>(fp, off, g->fused32);
+    merge_paths<float, float>(ap, off, g->apply32);
+  }
   merge_matvecs(mp, mv);
   cv_in.upload(cin);
   cv_res.upload(cres);
@@ -1092,14 +1102,14 @@ void Batch::run_factor(cudaStream_t s) {
     PhaseScope ps(prof, PH_CONVERT, s);
     launch_ew2d_batched<double, float>(cv_in.p, (int)cv_in.h.size(), t_in, false, s);
   }
-  run_path(prof, fused32, 0, info.p, s);
+  for (auto &g : groups) run_path(prof, g->fused32, 0, info.p, s);
   launch_ew2d_batched<float, double>(cv_x0.p, (int)cv_x0.h.size(), t_x0, false, s);
   residuals(s);
 }
 
 void Batch::run_sweep(cudaStream_t s) {
   launch_ew2d_batched<double, float>(cv_res.p, (int)cv_res.h.size(), t_res, false, s);
-  run_path(prof, apply32, 0, nullptr, s);
+  for (auto &g : groups) run_path(prof, g->apply32, 0, nullptr, s);
   launch_ew2d_batched<float, double>(add_y.p, (int)add_y.h.size(), t_x0, true, s);
   residuals(s);
 }

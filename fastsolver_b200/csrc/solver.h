@@ -234,7 +234,7 @@ struct System {
   int factored = -1;  // HODLR_PREC_* of the current factorization, -1 none
   int factored_form = 0;
   int red_chunk = 512;
-  int nb32 = 0;  // forced FP32 leaf panel width (0: by the largest leaf); batches align it
+  int nb32 = 0;  // forced FP32 leaf panel width (0: by the largest leaf)
   int bc_chunk = 512;
   int n_info = 0;
   Profiler prof;
@@ -275,18 +275,27 @@ struct System {
 // them.  The systems must outlive the batch and keep their sizes.
 struct Batch {
   std::vector<System *> sys;
-  PathPlan<float, float> fused32, apply32;
+  // Systems whose merged walk shares kernels: same FP32 leaf panel width and
+  // the same right-hand-side class (<= 16 or more columns: the skinny
+  // kernels' column tile).  Groups run back to back.
+  struct Group {
+    int nb = 0;
+    bool wide = false;
+    std::vector<int> members;
+    PathPlan<float, float> fused32, apply32;
+  };
+  std::vector<std::unique_ptr<Group>> groups;
   MatvecPlan mv;
   DevBuf<Ew2DTask<double, float>> cv_in, cv_res;  // D, B, U, V -> FP32; R64 -> Y32
   DevBuf<Ew2DTask<float, double>> cv_x0, add_y;   // X32 -> Xsol; Xsol += Y32
-  long long t_in = 0, t_res = 0, t_x0 = 0;        // largest tile count of each
+  long long t_in = 0, t_res = 0, t_x0 = 0;        // total tiles of each pass
   DevBuf<RatioTask> ratios;
   int max_m = 0;
   DevBuf<double> rr;            // column residual ratios, system k at rr_off[k]
   std::vector<int> rr_off;
   DevBuf<int> info;             // all systems' INFO slots, system k at info_off[k]
   std::vector<int> info_off;
-  int n_info = 0, nb = 0;
+  int n_info = 0;
   bool use_graphs = true;
   GraphSeg g_factor, g_sweep;
   Profiler prof;

@@ -61,23 +61,32 @@ __global__ void colratio_kernel(const double *__restrict__ r, long long ldr,
   }
 }
 
-// Batched element-wise pass: blockIdx.y picks the task, blockIdx.x strides
-// over its (column, 1024-row tile) pairs; each thread moves 4 rows of a tile,
-// consecutive threads on consecutive rows (coalesced on both sides).
+// Batched element-wise pass: one grid-stride loop over the tiles of all
+// tasks (a tile = 1024 rows of one column; tile -> task by binary search on
+// tile0), so large and small tasks share the grid evenly.  Each thread moves
+// 4 rows of a tile, consecutive threads on consecutive rows.
 template <typename TS, typename TD, bool ADD>
-__global__ void ew2d_batched_kernel(const Ew2DTask<TS, TD> *__restrict__ tasks) {
-  const Ew2DTask<TS, TD> tk = tasks[blockIdx.y];
-  const long long rtiles = cdiv<long long>(tk.rows, kEwTileRows);
-  const long long ntiles = rtiles * tk.cols;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const long long j = t / rtiles;
-    const long long i0 = (t - j * rtiles) * kEwTileRows;
+__global__ void ew2d_batched_kernel(const Ew2DTask<TS, TD> *__restrict__ tasks, int ntasks,
+                                    long long total) {
+  for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+    int lo = 0, hi = ntasks - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tasks[mid].tile0 <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const Ew2DTask<TS, TD> &tk = tasks[lo];
+    const long long rtiles = cdiv<long long>(tk.rows, kEwTileRows);
+    const long long lt = t - tk.tile0;
+    const long long j = lt / rtiles;
+    const long long i0 = (lt - j * rtiles) * kEwTileRows;
     const TS *src = tk.src + j * tk.lds;
     TD *dst = tk.dst + j * tk.ldd;
+    const long long rows = tk.rows;
 #pragma unroll
     for (int q = 0; q < kEwTileRows / kThreads; ++q) {
       const long long i = i0 + q * kThreads + threadIdx.x;
-      if (i < tk.rows) {
+      if (i < rows) {
         if (ADD) dst[i] += TD(src[i]);
         else dst[i] = TD(src[i]);
       }
@@ -325,14 +334,12 @@ void launch_colratio(const double *r, long long ldr, const double *b, long long 
 }
 
 template <typename TS, typename TD>
-void launch_ew2d_batched(const Ew2DTask<TS, TD> *tasks, int ntasks, long long max_tiles,
+void launch_ew2d_batched(const Ew2DTask<TS, TD> *tasks, int ntasks, long long total_tiles,
                          bool add, cudaStream_t s) {
-  if (ntasks <= 0 || max_tiles <= 0) return;
-  // about 8 resident CTAs of 256 threads per SM over all tasks
-  const long long want = std::max<long long>(1, 148LL * 8 / ntasks);
-  dim3 grid((unsigned)std::min<long long>(max_tiles, std::max<long long>(want, 4)), ntasks);
-  if (add) ew2d_batched_kernel<TS, TD, true><<<grid, kThreads, 0, s>>>(tasks);
-  else ew2d_batched_kernel<TS, TD, false><<<grid, kThreads, 0, s>>>(tasks);
+  if (ntasks <= 0 || total_tiles <= 0) return;
+  const unsigned grid = (unsigned)std::min<long long>(total_tiles, 148LL * 8);
+  if (add) ew2d_batched_kernel<TS, TD, true><<<grid, kThreads, 0, s>>>(tasks, ntasks, total_tiles);
+  else ew2d_batched_kernel<TS, TD, false><<<grid, kThreads, 0, s>>>(tasks, ntasks, total_tiles);
   HODLR_LAUNCH_CHECK();
 }
 template void launch_ew2d_batched<double, float>(const Ew2DTask<double, float> *, int, long long,

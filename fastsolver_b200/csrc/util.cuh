@@ -1,6 +1,7 @@
 // util.cuh -- element-wise kernels and device generators (util.cu).
 #pragma once
 #include <algorithm>
+#include <vector>
 
 #include "common.cuh"
 
@@ -56,7 +57,9 @@ void launch_gauss_fill_batched(const FillTask *tasks, int ntasks, long long max_
 void launch_scale_batched(const FillTask *tasks, int ntasks, long long max_elems, cudaStream_t s);
 
 // One block of a batched element-wise pass over column-major matrices:
-// dst(i, j) = TD(src(i, j)), or dst(i, j) += TD(src(i, j)).
+// dst(i, j) = TD(src(i, j)), or dst(i, j) += TD(src(i, j)).  The pass is cut
+// into tiles of kEwTileRows rows of one column; tile0 = tiles of the tasks
+// before this one (set by ew2d_prefix).
 template <typename TS, typename TD>
 struct Ew2DTask {
   const TS *src;
@@ -65,16 +68,25 @@ struct Ew2DTask {
   long long ldd;
   long long rows;
   long long cols;
+  long long tile0;
 };
-template <typename TS, typename TD>
-void launch_ew2d_batched(const Ew2DTask<TS, TD> *tasks, int ntasks, long long max_tiles,
-                         bool add, cudaStream_t s);
-// Row tiles of the batched pass (launch_ew2d_batched's max_tiles is the
-// largest of these over the tasks).
 constexpr int kEwTileRows = 1024;
 inline long long ew2d_tiles(long long rows, long long cols) {
   return cdiv<long long>(rows, kEwTileRows) * cols;
 }
+// Sets every task's tile0 and returns the total tile count.
+template <typename TS, typename TD>
+long long ew2d_prefix(std::vector<Ew2DTask<TS, TD>> &tasks) {
+  long long t = 0;
+  for (auto &k : tasks) {
+    k.tile0 = t;
+    t += ew2d_tiles(k.rows, k.cols);
+  }
+  return t;
+}
+template <typename TS, typename TD>
+void launch_ew2d_batched(const Ew2DTask<TS, TD> *tasks, int ntasks, long long total_tiles,
+                         bool add, cudaStream_t s);
 
 // Per-column residual ratios of one system of a batch:
 // out[c] = ||r(:, c)|| / ||b(:, c)||, c < cols.

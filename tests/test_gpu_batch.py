@@ -44,12 +44,36 @@ def test_batch_uneven_vs_oracle(fs, oracle, cuda):
     assert 1 <= it <= 4
     for (s, h), cfg, r in zip(pairs, SYSTEMS, rr):
         _check(oracle, s, h, cfg[1], r)
-    # one merged schedule: fewer launches than the systems solved one by one
+    # merged schedules: fewer launches than the systems solved one by one
     fs.reset_launch_count()
     for s, h in pairs:
         h.set_rhs(s.B)
         fs.FastSolver().solve_refined(h, fs.PREC_MIXED, tol=1e-12, maxiter=it)
-    assert launches < fs.launch_count() / 2
+    assert launches < fs.launch_count()
+
+
+def test_batch_launches_do_not_grow_with_systems(fs, oracle, cuda):
+    """Systems of one kernel class (same leaf panel width, <= 16 RHS) share
+    every launch: a batch of five costs the launches of its deepest member
+    plus the per-level steps the others add, not five solves."""
+    cfgs = [(8192, 4, 16, 512), (12000, 1, 40, 512), (20000, 16, 30, 400),
+            (6000, 8, 24, 512), (16384, 2, 50, 300)]
+    pairs = [_load(fs, oracle, *cfg, seed=500 + i) for i, cfg in enumerate(cfgs)]
+    single = []
+    for s, h in pairs:
+        fs.reset_launch_count()
+        it1, _ = fs.FastSolver().solve_refined(h, fs.PREC_MIXED, tol=0.0, maxiter=2,
+                                               check_conv=False)
+        single.append(fs.launch_count())
+    batch = fs.SystemBatch([h for _, h in pairs])
+    for s, h in pairs:
+        h.set_rhs(s.B)
+    fs.reset_launch_count()
+    it, rr = batch.solve_refined(tol=0.0, maxiter=2, check_conv=False)
+    assert it == 2
+    assert fs.launch_count() <= 1.2 * max(single)
+    for (s, h), cfg, r in zip(pairs, cfgs, rr):
+        _check(oracle, s, h, cfg[1], r)
 
 
 def test_batch_graph_replay_new_rhs(fs, oracle, cuda):
