@@ -513,32 +513,44 @@ __global__ void __launch_bounds__(kRegThreads, 1)
   }
 }
 
-// Row interchanges of panel `panel` on every column of D outside the panel
-// and on the leaf's X columns.  grid (column block, leaf); thread = column.
+// Row interchanges of panels [p0, p0 + np) (in order) on the D columns
+// [a0, a1) and [b0, b1) (clamped to the leaf) and, with with_x, on the
+// leaf's X columns.  grid (column block, leaf); thread = column.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-    leaf_laswp_kernel(const LeafFactorTask<T> *__restrict__ tasks, int k0, int panel, int nb) {
+    leaf_laswp_kernel(const LeafFactorTask<T> *__restrict__ tasks, int p0, int np, int nb,
+                      int a0, int a1, int b0, int b1, int with_x) {
   const LeafFactorTask<T> tk = tasks[blockIdx.y];
   const int n = tk.n;
-  if (k0 >= n || tk.swapflag[panel] == 0) return;
-  const int kb = min(nb, n - k0);
+  if (p0 * nb >= n) return;
+  bool any = false;
+  for (int q = p0; q < p0 + np && q * nb < n; ++q) any |= tk.swapflag[q] != 0;
+  if (!any) return;
+  const int na = max(0, min(a1, n) - a0);
+  const int nbr = max(0, min(b1, n) - b0);
   const int c = blockIdx.x * kThreads + threadIdx.x;
-  const int nd = n - kb;  // D columns outside the panel
   T *col;
-  if (c < nd) {
-    const int dc = c < k0 ? c : c + kb;
-    col = tk.D + (long long)dc * tk.ldd;
-  } else if (c < nd + tk.ncols) {
-    col = tk.X + (long long)(c - nd) * tk.ldx;
+  if (c < na) {
+    col = tk.D + (long long)(a0 + c) * tk.ldd;
+  } else if (c < na + nbr) {
+    col = tk.D + (long long)(b0 + c - na) * tk.ldd;
+  } else if (with_x && c < na + nbr + tk.ncols) {
+    col = tk.X + (long long)(c - na - nbr) * tk.ldx;
   } else {
     return;
   }
-  for (int j = 0; j < kb; ++j) {
-    const int p = tk.ipiv[k0 + j] - 1;
-    if (p != k0 + j) {
-      const T t = col[k0 + j];
-      col[k0 + j] = col[p];
-      col[p] = t;
+  for (int q = p0; q < p0 + np; ++q) {
+    const int k0 = q * nb;
+    if (k0 >= n) break;
+    if (tk.swapflag[q] == 0) continue;
+    const int kb = min(nb, n - k0);
+    for (int j = 0; j < kb; ++j) {
+      const int p = tk.ipiv[k0 + j] - 1;
+      if (p != k0 + j) {
+        const T t = col[k0 + j];
+        col[k0 + j] = col[p];
+        col[p] = t;
+      }
     }
   }
 }
@@ -794,11 +806,12 @@ void launch_leaf_panel(const LeafFactorTask<T> *tasks, int count, int max_n, int
 }
 
 template <typename T>
-void launch_leaf_laswp(const LeafFactorTask<T> *tasks, int count, int max_cols, int nb, int k0,
-                       int panel, cudaStream_t s) {
-  if (count <= 0 || max_cols <= 0) return;
+void launch_leaf_laswp(const LeafFactorTask<T> *tasks, int count, int max_cols, int nb, int p0,
+                       int np, int a0, int a1, int b0, int b1, bool with_x, cudaStream_t s) {
+  if (count <= 0 || max_cols <= 0 || np <= 0) return;
   dim3 grid(cdiv(max_cols, kThreads), count);
-  leaf_laswp_kernel<T><<<grid, kThreads, 0, s>>>(tasks, k0, panel, nb);
+  leaf_laswp_kernel<T><<<grid, kThreads, 0, s>>>(tasks, p0, np, nb, a0, a1, b0, b1,
+                                                 with_x ? 1 : 0);
   HODLR_LAUNCH_CHECK();
 }
 
@@ -838,8 +851,8 @@ template void launch_leaf_panel<double>(const LeafFactorTask<double> *, int, int
 template void launch_leaf_panel<float>(const LeafFactorTask<float> *, int, int, int, int, int,
                                        int *, cudaStream_t);
 template void launch_leaf_laswp<double>(const LeafFactorTask<double> *, int, int, int, int, int,
-                                        cudaStream_t);
+                                        int, int, int, int, bool, cudaStream_t);
 template void launch_leaf_laswp<float>(const LeafFactorTask<float> *, int, int, int, int, int,
-                                       cudaStream_t);
+                                       int, int, int, int, bool, cudaStream_t);
 
 }  // namespace hodlr

@@ -42,9 +42,11 @@ void launch_leaf_init(const LeafFactorTask<T> *tasks, int count, int *info, cuda
 template <typename T>
 void launch_leaf_panel(const LeafFactorTask<T> *tasks, int count, int max_n, int nb, int k0,
                        int panel, int *info, cudaStream_t s);
-// max_cols: largest n + ncols over the leaves
+// Row interchanges of panels [p0, p0 + np) on the D columns [a0, a1) and
+// [b0, b1) (clamped to each leaf's n) and, with with_x, on X.  max_cols:
+// an upper bound of the columns touched in any leaf (e.g. largest n + ncols).
 template <typename T>
-void launch_leaf_laswp(const LeafFactorTask<T> *tasks, int count, int max_cols, int nb, int k0,
-                       int panel, cudaStream_t s);
+void launch_leaf_laswp(const LeafFactorTask<T> *tasks, int count, int max_cols, int nb, int p0,
+                       int np, int a0, int a1, int b0, int b1, bool with_x, cudaStream_t s);
 
 }  // namespace hodlr

@@ -47,6 +47,7 @@ struct PathSpec {
   NodeStore *ns = nullptr;
   const LeafPlan<T> *factors = nullptr;  // apply paths: the blocked leaf factors
   int nb_force = 0;                      // leaf panel width (0: by the largest leaf)
+  int ob = 0;                            // leaf outer block width (0: one level)
   bool factor = false;
   int red_chunk = 512, bc_chunk = 512;
 };
@@ -83,19 +84,25 @@ void path_need(const Tree &t, bool factor, int chunk, size_t &part, size_t &wfin
 }
 
 
-// Per-panel GEMM item lists of the blocked leaf factorization (see
+// Step lists of the two-level blocked leaf factorization (see LeafPlan and
 // leaf_blocked.cu): forward steps on [D | X], then the backward solve on X.
+// Every step is one merged launch over all leaves; a leaf without work in a
+// step contributes no item.
 template <typename T>
 void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long ldx,
                      int *ipiv, int *perm, bool factor_cols_all, int m, LeafPlan<T> &lp,
-                     int nb_force) {
+                     int nb_force, int ob_req) {
+  using Step = typename LeafPlan<T>::Step;
   const int nleaf = (int)t.leaves.size();
-  int max_panels = 0;
   lp.max_n = 0;
   for (int id : t.leaves) lp.max_n = std::max(lp.max_n, t.nodes[id].nrow);
   const int NB = nb_force > 0 ? nb_force : leaf_nb<T>(lp.max_n);
+  const int OB = ob_req >= NB ? ob_req / NB * NB : NB;
+  const int P = OB / NB;
   lp.nb = NB;
-  for (int id : t.leaves) max_panels = std::max(max_panels, cdiv(t.nodes[id].nrow, NB));
+  lp.ob = OB;
+  const int max_panels = cdiv(lp.max_n, NB);
+  lp.nblocks = cdiv(lp.max_n, OB);
   lp.Linv.ensure((size_t)nleaf * max_panels * NB * NB);
   lp.Uinv.ensure((size_t)nleaf * max_panels * NB * NB);
   lp.swapflag.ensure((size_t)nleaf * max_panels);
@@ -123,73 +130,125 @@ void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long
   lp.nleaf = nleaf;
   lp.fwd.clear();
   lp.bwd.clear();
-  for (int pi = 0; pi < max_panels; ++pi) {
-    const int k0 = pi * NB;
-    auto F = std::make_unique<typename LeafPlan<T>::Fwd>();
-    F->k0 = k0;
-    F->panel = pi;
-    std::vector<GemmItem<T, T>> ti, ui;
-    std::vector<GemmSeg<T>> ts, us;
-    for (int q = 0; q < nleaf; ++q) {
-      const LeafFactorTask<T> &k = tasks[q];
-      if (k0 >= k.n) continue;
-      const int kb = std::min(NB, k.n - k0);
-      const int rest = k.n - k0 - kb;
-      const T *Li = k.Linv + (size_t)pi * NB * NB;
-      // U12 = L11^{-1} A12 in place: D columns right of the panel, X columns
-      auto trsm = [&](T *C, long long ldc, int N) {
-        if (N <= 0) return;
-        GemmSeg<T> g{Li, C, NB, ldc, kb, 0};
-        GemmItem<T, T> it{C, nullptr, ldc, 0, kb, N, (int)ts.size(), 1};
-        ts.push_back(g);
-        ti.push_back(it);
-      };
-      trsm(k.D + k0 + (long long)(k0 + kb) * ldd, ldd, rest);
-      trsm(k.X + k0, ldx, k.ncols);
-      if (rest > 0) {
-        const T *L21 = k.D + (k0 + kb) + (long long)k0 * ldd;
-        auto upd = [&](T *C, long long ldc, const T *B, long long ldb, int N) {
-          if (N <= 0) return;
-          GemmSeg<T> g{L21, B, ldd, ldb, kb, 0};
-          GemmItem<T, T> it{C, C, ldc, ldc, rest, N, (int)us.size(), 1};
-          us.push_back(g);
-          ui.push_back(it);
-        };
-        upd(k.D + (k0 + kb) + (long long)(k0 + kb) * ldd, ldd,
-            k.D + k0 + (long long)(k0 + kb) * ldd, ldd, rest);
-        upd(k.X + (k0 + kb), ldx, k.X + k0, ldx, k.ncols);
-      }
+  // item lists of one GEMM step, filled leaf by leaf
+  struct Acc {
+    std::vector<GemmItem<T, T>> it;
+    std::vector<GemmSeg<T>> sg;
+    void add(T *C, long long ldc, int M, int N, const T *A, long long lda, const T *B,
+             long long ldb, int K, bool inplace) {
+      if (M <= 0 || N <= 0 || K <= 0) return;
+      GemmSeg<T> g{A, B, lda, ldb, K, 0};
+      GemmItem<T, T> i{C, inplace ? C : nullptr, ldc, inplace ? ldc : 0, M, N, (int)sg.size(), 1};
+      sg.push_back(g);
+      it.push_back(i);
     }
-    F->trsm.set(ti, ts);
-    F->update.set(ui, us);
-    lp.fwd.push_back(std::move(F));
-  }
-  for (int pi = max_panels - 1; pi >= 0; --pi) {
-    const int k0 = pi * NB;
-    auto B = std::make_unique<typename LeafPlan<T>::Bwd>();
-    std::vector<GemmItem<T, T>> ti, ui;
-    std::vector<GemmSeg<T>> ts, us;
-    for (int q = 0; q < nleaf; ++q) {
-      const LeafFactorTask<T> &k = tasks[q];
-      if (k0 >= k.n || k.ncols <= 0) continue;
-      const int kb = std::min(NB, k.n - k0);
-      const T *Ui = k.Uinv + (size_t)pi * NB * NB;
-      T *Xk = k.X + k0;
-      GemmSeg<T> g{Ui, Xk, NB, ldx, kb, 0};
-      GemmItem<T, T> it{Xk, nullptr, ldx, 0, kb, k.ncols, (int)ts.size(), 1};
-      ts.push_back(g);
-      ti.push_back(it);
-      if (k0 > 0) {
-        GemmSeg<T> g2{k.D + (long long)k0 * ldd, Xk, ldd, ldx, kb, 0};
-        GemmItem<T, T> it2{k.X, k.X, ldx, ldx, k0, k.ncols, (int)us.size(), 1};
-        us.push_back(g2);
-        ui.push_back(it2);
+  };
+  auto gemm_step = [&](typename LeafPlan<T>::Kind kind, const Acc &a) {
+    auto st = std::make_unique<Step>();
+    st->kind = kind;
+    st->g.set(a.it, a.sg);
+    return st;
+  };
+  auto laswp_step = [&](int p0, int np, int a0, int a1, int b0, int b1, bool with_x) {
+    auto st = std::make_unique<Step>();
+    st->kind = LeafPlan<T>::kLaswp;
+    st->panel = p0;
+    st->np = np;
+    st->a0 = a0; st->a1 = a1; st->b0 = b0; st->b1 = b1;
+    st->with_x = with_x;
+    return st;
+  };
+  constexpr int kAll = 1 << 30;
+  for (int J = 0; J < lp.nblocks; ++J) {
+    const int j0 = J * OB;
+    // the block's panels: factor, interchange and update inside the block columns
+    for (int p = 0; p < P; ++p) {
+      const int pi = J * P + p, k0 = pi * NB;
+      auto pan = std::make_unique<Step>();
+      pan->kind = LeafPlan<T>::kPanel;
+      pan->k0 = k0;
+      pan->panel = pi;
+      lp.fwd.push_back(std::move(pan));
+      lp.fwd.push_back(laswp_step(pi, 1, j0, k0, k0 + NB, j0 + OB, false));
+      Acc tr, up;
+      for (const LeafFactorTask<T> &k : tasks) {
+        if (k0 >= k.n) continue;
+        const int kb = std::min(NB, k.n - k0);
+        const int N = std::min(j0 + OB, k.n) - (k0 + kb);
+        const int rest = k.n - k0 - kb;
+        const T *Li = k.Linv + (size_t)pi * NB * NB;
+        T *U12 = k.D + k0 + (long long)(k0 + kb) * ldd;
+        tr.add(U12, ldd, kb, N, Li, NB, U12, ldd, kb, false);
+        up.add(k.D + (k0 + kb) + (long long)(k0 + kb) * ldd, ldd, rest, N,
+               k.D + (k0 + kb) + (long long)k0 * ldd, ldd, U12, ldd, kb, true);
       }
+      lp.fwd.push_back(gemm_step(LeafPlan<T>::kTrsm, tr));
+      lp.fwd.push_back(gemm_step(LeafPlan<T>::kUpdate, up));
     }
-    B->trsm.set(ti, ts);
-    B->update.set(ui, us);
-    lp.bwd.push_back(std::move(B));
+    // the block's interchanges on the columns left and right of it and on X
+    lp.fwd.push_back(laswp_step(J * P, P, 0, j0, j0 + OB, kAll, true));
+    // block rows: U12 = L11^{-1} A12 by panels on R = (D right of the block | X)
+    for (int p = 0; p < P; ++p) {
+      const int pi = J * P + p, k0 = pi * NB;
+      Acc tr, up;
+      for (const LeafFactorTask<T> &k : tasks) {
+        if (k0 >= k.n) continue;
+        const int kb = std::min(NB, k.n - k0);
+        const int obe = std::min(OB, k.n - j0);
+        const int nd = k.n - j0 - obe;           // D columns right of the block
+        const int below = j0 + obe - k0 - kb;    // block rows below this panel
+        const T *Li = k.Linv + (size_t)pi * NB * NB;
+        T *Dr = k.D + k0 + (long long)(j0 + obe) * ldd;
+        T *Xr = k.X + k0;
+        tr.add(Dr, ldd, kb, nd, Li, NB, Dr, ldd, kb, false);
+        tr.add(Xr, ldx, kb, k.ncols, Li, NB, Xr, ldx, kb, false);
+        const T *L = k.D + (k0 + kb) + (long long)k0 * ldd;
+        up.add(Dr + kb, ldd, below, nd, L, ldd, Dr, ldd, kb, true);
+        up.add(Xr + kb, ldx, below, k.ncols, L, ldd, Xr, ldx, kb, true);
+      }
+      lp.fwd.push_back(gemm_step(LeafPlan<T>::kTrsm, tr));
+      lp.fwd.push_back(gemm_step(LeafPlan<T>::kUpdate, up));
+    }
+    // trailing update of depth OB: A22 -= L21 U12 on R, rows below the block
+    Acc big;
+    for (const LeafFactorTask<T> &k : tasks) {
+      if (j0 >= k.n) continue;
+      const int obe = std::min(OB, k.n - j0);
+      const int rest = k.n - j0 - obe;
+      const T *L21 = k.D + (j0 + obe) + (long long)j0 * ldd;
+      big.add(k.D + (j0 + obe) + (long long)(j0 + obe) * ldd, ldd, rest, rest, L21, ldd,
+              k.D + j0 + (long long)(j0 + obe) * ldd, ldd, obe, true);
+      big.add(k.X + (j0 + obe), ldx, rest, k.ncols, L21, ldd, k.X + j0, ldx, obe, true);
+    }
+    lp.fwd.push_back(gemm_step(LeafPlan<T>::kUpdate, big));
   }
+  lp.fwd_per_block = 6 * P + 2;
+  // backward solve on X, last block first
+  for (int J = lp.nblocks - 1; J >= 0; --J) {
+    const int j0 = J * OB;
+    for (int p = P - 1; p >= 0; --p) {
+      const int pi = J * P + p, k0 = pi * NB;
+      Acc tr, up;
+      for (const LeafFactorTask<T> &k : tasks) {
+        if (k0 >= k.n) continue;
+        const int kb = std::min(NB, k.n - k0);
+        T *Xk = k.X + k0;
+        tr.add(Xk, ldx, kb, k.ncols, k.Uinv + (size_t)pi * NB * NB, NB, Xk, ldx, kb, false);
+        up.add(k.X + j0, ldx, k0 - j0, k.ncols, k.D + j0 + (long long)k0 * ldd, ldd, Xk, ldx,
+               kb, true);
+      }
+      lp.bwd.push_back(gemm_step(LeafPlan<T>::kTrsm, tr));
+      lp.bwd.push_back(gemm_step(LeafPlan<T>::kUpdate, up));
+    }
+    Acc big;
+    for (const LeafFactorTask<T> &k : tasks) {
+      if (j0 >= k.n) continue;
+      const int obe = std::min(OB, k.n - j0);
+      big.add(k.X, ldx, j0, k.ncols, k.D + (long long)j0 * ldd, ldd, k.X + j0, ldx, obe, true);
+    }
+    lp.bwd.push_back(gemm_step(LeafPlan<T>::kUpdate, big));
+  }
+  lp.bwd_per_block = 2 * P + 1;
 }
 
 template <typename TA, typename TC, typename TACC>
@@ -228,7 +287,7 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
   plan.leaf_tasks.upload(lt);
   if (sp.factor) {
     build_leaf_plan<T>(t, sp.D, sp.ldd, sp.X, sp.ldx, sp.ipiv, sp.perm, true, m, plan.leaf,
-                       sp.nb_force);
+                       sp.nb_force, sp.ob);
   } else if (sp.factors) {
     std::vector<LeafFactorTask<T>> at = sp.factors->host_tasks;
     for (size_t q = 0; q < at.size(); ++q) {
@@ -440,31 +499,46 @@ struct PhaseScope {
 
 template <typename T>
 void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t s) {
+  using Step = typename LeafPlan<T>::Step;
+  auto run_step = [&](const Step &st) {
+    switch (st.kind) {
+      case LeafPlan<T>::kPanel: {
+        PhaseScope pp(pf, PH_LEAF_PANEL, s);
+        launch_leaf_panel<T>(lp.tasks.p, lp.nleaf, lp.max_n, lp.nb, st.k0, st.panel, info, s);
+        break;
+      }
+      case LeafPlan<T>::kLaswp: {
+        if (st.a1 <= st.a0 && st.b1 <= st.b0 && !st.with_x) break;  // no columns
+        PhaseScope pp(pf, PH_LEAF_PANEL, s);
+        launch_leaf_laswp<T>(lp.tasks.p, lp.nleaf, lp.laswp_cols, lp.nb, st.panel, st.np, st.a0,
+                             st.a1, st.b0, st.b1, st.with_x, s);
+        break;
+      }
+      case LeafPlan<T>::kTrsm: {
+        if (st.g.n == 0) break;
+        PhaseScope pt(pf, PH_LEAF_TRSM, s);
+        run_gemm<T, T, T>(st.g, false, T(1), T(0), s);
+        break;
+      }
+      case LeafPlan<T>::kUpdate: {
+        if (st.g.n == 0) break;
+        PhaseScope pu(pf, PH_LEAF_UPDATE, s);
+        run_gemm<T, T, T>(st.g, false, T(-1), T(1), s);
+        break;
+      }
+    }
+  };
   {
     PhaseScope ps(pf, PH_GETRF, s);
     launch_leaf_init<T>(lp.tasks.p, lp.nleaf, info, s);
-    for (const auto &F : lp.fwd) {
-      {
-        PhaseScope pp(pf, PH_LEAF_PANEL, s);
-        launch_leaf_panel<T>(lp.tasks.p, lp.nleaf, lp.max_n, lp.nb, F->k0, F->panel, info, s);
-        launch_leaf_laswp<T>(lp.tasks.p, lp.nleaf, lp.laswp_cols, lp.nb, F->k0, F->panel, s);
-      }
-      if (F->trsm.n > 0) {
-        PhaseScope pt(pf, PH_LEAF_TRSM, s);
-        run_gemm<T, T, T>(F->trsm, false, T(1), T(0), s);
-      }
-      if (F->update.n > 0) {
-        PhaseScope pu(pf, PH_LEAF_UPDATE, s);
-        run_gemm<T, T, T>(F->update, false, T(-1), T(1), s);
-      }
-    }
+    for (const auto &st : lp.fwd) run_step(*st);
   }
   {
     PhaseScope ps(pf, PH_GETRS, s);
-    for (const auto &B : lp.bwd) {
-      run_gemm<T, T, T>(B->trsm, false, T(1), T(0), s);
-      run_gemm<T, T, T>(B->update, false, T(-1), T(1), s);
-    }
+    for (const auto &st : lp.bwd)
+      if (st->g.n > 0)
+        run_gemm<T, T, T>(st->g, false, st->kind == LeafPlan<T>::kTrsm ? T(1) : T(-1),
+                          st->kind == LeafPlan<T>::kTrsm ? T(0) : T(1), s);
   }
 }
 
@@ -664,56 +738,63 @@ struct ItemAcc {
 template <typename T>
 void merge_leaf_plans(const std::vector<const LeafPlan<T> *> &src, const std::vector<int> &info_off,
                       LeafPlan<T> &dst) {
+  using Step = typename LeafPlan<T>::Step;
   std::vector<LeafFactorTask<T>> tasks;
   dst.max_n = dst.laswp_cols = 0;
   dst.nb = src.empty() ? 0 : src[0]->nb;
-  size_t panels = 0;
+  dst.ob = src.empty() ? 0 : src[0]->ob;
+  dst.nblocks = 0;
   for (size_t k = 0; k < src.size(); ++k) {
     const LeafPlan<T> &lp = *src[k];
-    if (lp.nb != dst.nb) throw CudaError{cudaErrorInvalidValue};
+    if (lp.nb != dst.nb || lp.ob != dst.ob) throw CudaError{cudaErrorInvalidValue};
     for (LeafFactorTask<T> t : lp.host_tasks) {
       t.info_slot += info_off[k];
       tasks.push_back(t);
     }
     dst.max_n = std::max(dst.max_n, lp.max_n);
     dst.laswp_cols = std::max(dst.laswp_cols, lp.laswp_cols);
-    panels = std::max(panels, lp.fwd.size());
+    dst.nblocks = std::max(dst.nblocks, lp.nblocks);
   }
+  dst.fwd_per_block = src[0]->fwd_per_block;
+  dst.bwd_per_block = src[0]->bwd_per_block;
   dst.tasks.upload(tasks);
   dst.host_tasks = tasks;
   dst.nleaf = (int)tasks.size();
   dst.fwd.clear();
   dst.bwd.clear();
-  for (size_t pi = 0; pi < panels; ++pi) {
-    auto F = std::make_unique<typename LeafPlan<T>::Fwd>();
-    F->k0 = (int)pi * dst.nb;
-    F->panel = (int)pi;
-    ItemAcc<T, T> tr, up;
-    for (const LeafPlan<T> *lp : src) {
-      if (pi >= lp->fwd.size()) continue;
-      tr.add(lp->fwd[pi]->trsm);
-      up.add(lp->fwd[pi]->update);
+  // the step lists have the same shape per block in every system (same nb
+  // and ob): step i of block J merges the systems that have block J; the
+  // backward lists start at each system's own last block
+  auto merge_step = [&](const Step &proto, const std::vector<const Step *> &parts) {
+    auto st = std::make_unique<Step>();
+    st->kind = proto.kind;
+    st->k0 = proto.k0;
+    st->panel = proto.panel;
+    st->np = proto.np;
+    st->a0 = proto.a0; st->a1 = proto.a1; st->b0 = proto.b0; st->b1 = proto.b1;
+    st->with_x = proto.with_x;
+    if (proto.kind == LeafPlan<T>::kTrsm || proto.kind == LeafPlan<T>::kUpdate) {
+      ItemAcc<T, T> acc;
+      for (const Step *p : parts) acc.add(p->g);
+      acc.store(st->g);
     }
-    tr.store(F->trsm);
-    up.store(F->update);
-    dst.fwd.push_back(std::move(F));
-  }
-  // backward steps run from the last panel to the first; a system's bwd[j]
-  // is its panel fwd.size() - 1 - j
-  for (size_t j = 0; j < panels; ++j) {
-    const size_t pi = panels - 1 - j;
-    auto B = std::make_unique<typename LeafPlan<T>::Bwd>();
-    ItemAcc<T, T> tr, up;
-    for (const LeafPlan<T> *lp : src) {
-      if (pi >= lp->fwd.size()) continue;
-      const size_t jj = lp->fwd.size() - 1 - pi;
-      tr.add(lp->bwd[jj]->trsm);
-      up.add(lp->bwd[jj]->update);
+    return st;
+  };
+  for (int J = 0; J < dst.nblocks; ++J)
+    for (int i = 0; i < dst.fwd_per_block; ++i) {
+      std::vector<const Step *> parts;
+      for (const LeafPlan<T> *lp : src)
+        if (J < lp->nblocks) parts.push_back(lp->fwd[(size_t)J * dst.fwd_per_block + i].get());
+      dst.fwd.push_back(merge_step(*parts[0], parts));
     }
-    tr.store(B->trsm);
-    up.store(B->update);
-    dst.bwd.push_back(std::move(B));
-  }
+  for (int J = dst.nblocks - 1; J >= 0; --J)
+    for (int i = 0; i < dst.bwd_per_block; ++i) {
+      std::vector<const Step *> parts;
+      for (const LeafPlan<T> *lp : src)
+        if (J < lp->nblocks)
+          parts.push_back(lp->bwd[(size_t)(lp->nblocks - 1 - J) * dst.bwd_per_block + i].get());
+      dst.bwd.push_back(merge_step(*parts[0], parts));
+    }
 }
 
 // Level j of the merged plan is level j (deepest first) of every system
@@ -892,7 +973,7 @@ void System::ensure_fp64() {
     f.X = X64.p; f.ldx = N; f.Usrc = X64.p; f.ldu = N;
     f.D = DLU64.p; f.ldd = N; f.ipiv = ipiv64.p; f.perm = perm64.p;
     f.V = V.p; f.ldv = N; f.part = part64.p; f.wfin = wfin64.p; f.eta = eta64.p; f.M = ns64.M64.p; f.ns = &ns64;
-    f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk;
+    f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk; f.ob = ob64;
     build_path(tree, f, fused64[form], form);
     PathSpec<double, double> a = f;
     a.X = Y64.p; a.factor = false; a.factors = &fused64[form].leaf;
@@ -921,6 +1002,7 @@ void System::ensure_mixed() {
   f.D = D32.p; f.ldd = N; f.ipiv = ipiv32.p; f.perm = perm32.p;
   f.V = V32.p; f.ldv = N; f.part = part32.p; f.wfin = wfin32.p; f.eta = eta32.p; f.M = ns32.M32.p; f.ns = &ns32;
   f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk; f.nb_force = nb32;
+  f.ob = ob32;
   build_path(tree, f, fused32, 0);
   PathSpec<float, float> a = f;
   a.X = Y32.p; a.factor = false; a.factors = &fused32.leaf;
@@ -1011,15 +1093,16 @@ void Batch::build(const std::vector<System *> &systems) {
   for (size_t k = 0; k < sys.size(); ++k) {
     System *S = sys[k];
     S->ensure_mixed();
-    const int nbk = S->fused32.leaf.nb;
+    const int nbk = S->fused32.leaf.nb, obk = S->fused32.leaf.ob;
     const bool wide = S->m > 16;
     Group *g = nullptr;
     for (auto &q : groups)
-      if (q->nb == nbk && q->wide == wide) g = q.get();
+      if (q->nb == nbk && q->ob == obk && q->wide == wide) g = q.get();
     if (!g) {
       groups.push_back(std::make_unique<Group>());
       g = groups.back().get();
       g->nb = nbk;
+      g->ob = obk;
       g->wide = wide;
     }
     g->members.push_back((int)k);

@@ -96,23 +96,32 @@ struct GemmLaunch {
   }
 };
 
-// Blocked factorization of every leaf on [D | X] (leaf_blocked.cu).
+// Blocked factorization of every leaf on [D | X] (leaf_blocked.cu), two
+// levels: outer blocks of `ob` columns, each factored as ob / nb register
+// panels whose row interchanges and updates stay inside the block's columns;
+// then the block's interchanges on the other columns, the block-row solve
+// and one trailing update of depth ob.  The backward solve on X runs by the
+// same blocks.  ob == nb is the one-level right-looking factorization.
 template <typename T>
 struct LeafPlan {
   DevBuf<LeafFactorTask<T>> tasks;
   DevBuf<T> Linv, Uinv;
   DevBuf<int> swapflag;
   std::vector<LeafFactorTask<T>> host_tasks;  // for apply plans with these factors
-  int nleaf = 0, max_n = 0, laswp_cols = 0, nb = 0;
-  struct Fwd {
-    int k0, panel;
-    GemmLaunch<T, T> trsm, update;
+  int nleaf = 0, max_n = 0, laswp_cols = 0, nb = 0, ob = 0;
+  enum Kind { kPanel, kLaswp, kTrsm, kUpdate };
+  struct Step {
+    Kind kind = kPanel;
+    int k0 = 0, panel = 0;          // kPanel: the panel; kLaswp: first panel
+    int np = 0;                     // kLaswp: panels applied
+    int a0 = 0, a1 = 0, b0 = 0, b1 = 0;  // kLaswp: D column ranges (clamped per leaf)
+    bool with_x = false;            // kLaswp: X columns too
+    GemmLaunch<T, T> g;             // kTrsm (C = A B) / kUpdate (C -= A B)
   };
-  struct Bwd {
-    GemmLaunch<T, T> trsm, update;
-  };
-  std::vector<std::unique_ptr<Fwd>> fwd;
-  std::vector<std::unique_ptr<Bwd>> bwd;
+  // fwd: the steps of block 0, then block 1, ... (fwd_per_block each);
+  // bwd: the steps of the last block first (bwd_per_block each)
+  std::vector<std::unique_ptr<Step>> fwd, bwd;
+  int nblocks = 0, fwd_per_block = 0, bwd_per_block = 0;
 };
 
 template <typename T, typename TE>
@@ -235,6 +244,7 @@ struct System {
   int factored_form = 0;
   int red_chunk = 512;
   int nb32 = 0;  // forced FP32 leaf panel width (0: by the largest leaf)
+  int ob32 = 128, ob64 = 0;  // leaf outer block width per path (0: one level)
   int bc_chunk = 512;
   int n_info = 0;
   Profiler prof;
@@ -279,7 +289,7 @@ struct Batch {
   // the same right-hand-side class (<= 16 or more columns: the skinny
   // kernels' column tile).  Groups run back to back.
   struct Group {
-    int nb = 0;
+    int nb = 0, ob = 0;
     bool wide = false;
     std::vector<int> members;
     PathPlan<float, float> fused32, apply32;
