@@ -81,10 +81,34 @@ _SIGS = {
     "hodlr_batch_solve_refined": [_vp, _d, _i, _ip, _dp, _dp, _ip, _vp],
     "hodlr_batch_set_profiling": [_vp, _i],
     "hodlr_batch_phase_times": [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), _i],
+    "hodlr_get_schedule": [_vp, _vp],
+    "hodlr_set_schedule": [_vp, _vp],
+    "hodlr_autotune": [_vp, _i, _d, _i, _vp, _dp, _vp, _i, _ip],
+    "hodlr_batch_autotune": [_vp, _d, _i, _vp, _dp, _vp, _i, _ip],
     "hodlr_launch_count": [],
     "hodlr_reset_launch_count": [],
     "hodlr_status_string": [_i],
 }
+
+
+class Schedule(ctypes.Structure):
+    """hodlr_schedule (include/hodlr_gpu.h)."""
+    _fields_ = [("leaf_nb", ctypes.c_int), ("leaf_ob32", ctypes.c_int),
+                ("leaf_ob64", ctypes.c_int), ("reduce_rows", ctypes.c_int),
+                ("bcast_rows", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "Schedule":
+        return cls(**{k: int(d[k]) for k, _ in cls._fields_})
+
+
+class TuneTrial(ctypes.Structure):
+    """hodlr_tune_trial (include/hodlr_gpu.h)."""
+    _fields_ = [("schedule", Schedule), ("ms", ctypes.c_double)]
+
 
 for _name, _args in _SIGS.items():
     _f = getattr(lib, _name)

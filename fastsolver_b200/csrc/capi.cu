@@ -1,4 +1,5 @@
 // capi.cu -- the extern "C" entry points declared in include/hodlr_gpu.h.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -761,6 +762,60 @@ int hodlr_solve(hodlr_system h, hodlr_stream_t stream) {
   });
 }
 
+// The refined solve of one system on stream s (see hodlr_solve_refined).
+static int refined_body(System &S, int precision, double tol, int maxiter, int *iters,
+                        double *relres, cudaStream_t s) {
+  const long long N = S.N;
+  const size_t nm = (size_t)N * S.m;
+  // two replayable segments: factor pass + residual, and one refinement
+  // sweep + residual (captured as CUDA graphs on the first call)
+  if (precision == HODLR_PREC_MIXED) {
+    S.ensure_mixed();
+    S.run_graph(S.g_factor32, s, [&]() {
+      S.run_factor32(s);
+      launch_convert2d<float, double>(S.X32.p, N, S.Xsol.p, N, N, S.m, s);
+      S.relres_enqueue(s);
+    });
+    S.factored = HODLR_PREC_MIXED;  // (host state is not part of a replay)
+    S.factored_form = 0;
+  } else {
+    S.ensure_fp64();
+    S.run_graph(S.g_factor64, s, [&]() {
+      S.run_fused64(0, s);
+      S.relres_enqueue(s);
+    });
+    S.factored = HODLR_PREC_FP64;
+    S.factored_form = 0;
+  }
+  int info = S.check_info(s);
+  if (info) return info;
+  int it = 0;
+  double rr = S.relres_read(s);
+  while (rr > tol && it < maxiter) {
+    if (precision == HODLR_PREC_MIXED) {
+      S.run_graph(S.g_sweep32, s, [&]() {
+        launch_convert2d<double, float>(S.R64.p, N, S.Y32.p, N, N, S.m, s);
+        S.run_apply32(s);
+        launch_add2d<float>(S.Xsol.p, N, S.Y32.p, N, N, S.m, s);
+        S.relres_enqueue(s);
+      });
+    } else {
+      S.run_graph(S.g_sweep64, s, [&]() {
+        HODLR_CUDA_TRY(cudaMemcpyAsync(S.Y64.p, S.R64.p, sizeof(double) * nm,
+                                       cudaMemcpyDeviceToDevice, s));
+        S.run_apply64(s);
+        launch_add2d<double>(S.Xsol.p, N, S.Y64.p, N, N, S.m, s);
+        S.relres_enqueue(s);
+      });
+    }
+    ++it;
+    rr = S.relres_read(s);
+  }
+  if (iters) *iters = it;
+  if (relres) *relres = rr;
+  return rr <= tol ? 0 : HODLR_ERR_NOCONV;
+}
+
 int hodlr_solve_refined(hodlr_system h, int precision, double tol, int maxiter, int *iters,
                         double *relres, hodlr_stream_t stream) {
   if (!h) return -1;
@@ -768,57 +823,199 @@ int hodlr_solve_refined(hodlr_system h, int precision, double tol, int maxiter, 
   if (!(tol >= 0.0)) return -3;
   if (maxiter < 0) return -4;
   return guarded([&]() -> int {
-    System &S = h->sys;
-    cudaStream_t s = as_stream(stream);
-    const long long N = S.N;
-    const size_t nm = (size_t)N * S.m;
-    // two replayable segments: factor pass + residual, and one refinement
-    // sweep + residual (captured as CUDA graphs on the first call)
-    if (precision == HODLR_PREC_MIXED) {
-      S.ensure_mixed();
-      S.run_graph(S.g_factor32, s, [&]() {
-        S.run_factor32(s);
-        launch_convert2d<float, double>(S.X32.p, N, S.Xsol.p, N, N, S.m, s);
-        S.relres_enqueue(s);
-      });
-      S.factored = HODLR_PREC_MIXED;  // (host state is not part of a replay)
-      S.factored_form = 0;
-    } else {
-      S.ensure_fp64();
-      S.run_graph(S.g_factor64, s, [&]() {
-        S.run_fused64(0, s);
-        S.relres_enqueue(s);
-      });
-      S.factored = HODLR_PREC_FP64;
-      S.factored_form = 0;
-    }
-    int info = S.check_info(s);
-    if (info) return info;
-    int it = 0;
-    double rr = S.relres_read(s);
-    while (rr > tol && it < maxiter) {
-      if (precision == HODLR_PREC_MIXED) {
-        S.run_graph(S.g_sweep32, s, [&]() {
-          launch_convert2d<double, float>(S.R64.p, N, S.Y32.p, N, N, S.m, s);
-          S.run_apply32(s);
-          launch_add2d<float>(S.Xsol.p, N, S.Y32.p, N, N, S.m, s);
-          S.relres_enqueue(s);
-        });
-      } else {
-        S.run_graph(S.g_sweep64, s, [&]() {
-          HODLR_CUDA_TRY(cudaMemcpyAsync(S.Y64.p, S.R64.p, sizeof(double) * nm,
-                                         cudaMemcpyDeviceToDevice, s));
-          S.run_apply64(s);
-          launch_add2d<double>(S.Xsol.p, N, S.Y64.p, N, N, S.m, s);
-          S.relres_enqueue(s);
-        });
+    return refined_body(h->sys, precision, tol, maxiter, iters, relres, as_stream(stream));
+  });
+}
+
+// ---------------------------------------------------------------------------
+// launch schedule and its autotuner
+// ---------------------------------------------------------------------------
+
+static hodlr_schedule schedule_of(const System &S) {
+  hodlr_schedule c{};
+  c.leaf_nb = S.nb32;
+  c.leaf_ob32 = S.ob32;
+  c.leaf_ob64 = S.ob64;
+  c.reduce_rows = S.red_chunk;
+  c.bcast_rows = S.bc_chunk;
+  return c;
+}
+
+// 0, or the negative index of the first invalid field (as an argument error)
+static int schedule_check(const System &S, const hodlr_schedule &c) {
+  if (c.leaf_nb != 0 && c.leaf_nb != 32 && c.leaf_nb != 64) return -2;
+  if (c.leaf_nb == 64 && S.nmax > 512) return -2;  // the 64-wide panel holds <= 512 rows
+  if (c.leaf_ob32 < 0 || c.leaf_ob32 > 1024) return -3;
+  if (c.leaf_ob64 < 0 || c.leaf_ob64 > 1024) return -4;
+  if (c.reduce_rows < 16 || c.reduce_rows > 65536 || c.reduce_rows % 16) return -5;
+  if (c.bcast_rows < 16 || c.bcast_rows > 65536 || c.bcast_rows % 16) return -6;
+  return 0;
+}
+
+// Installs a (checked) schedule: the launch plans and captured graphs are
+// rebuilt on the next solve, and the system must be factored again.
+static void schedule_apply(System &S, const hodlr_schedule &c) {
+  const hodlr_schedule cur = schedule_of(S);
+  if (std::memcmp(&cur, &c, sizeof(c)) == 0) return;
+  S.nb32 = c.leaf_nb;
+  S.ob32 = c.leaf_ob32;
+  S.ob64 = c.leaf_ob64;
+  S.red_chunk = c.reduce_rows;
+  S.bc_chunk = c.bcast_rows;
+  S.fused32.built = false;
+  S.fused64[0].built = S.fused64[1].built = false;
+  S.reset_graphs();
+  S.factored = -1;
+}
+
+int hodlr_get_schedule(hodlr_system h, hodlr_schedule *out) {
+  if (!h) return -1;
+  if (!out) return -2;
+  *out = schedule_of(h->sys);
+  return 0;
+}
+
+int hodlr_set_schedule(hodlr_system h, const hodlr_schedule *in) {
+  if (!h) return -1;
+  if (!in) return -2;
+  if (int rc = schedule_check(h->sys, *in)) return rc;
+  return guarded([&]() -> int {
+    schedule_apply(h->sys, *in);
+    return 0;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Coordinate search over the schedule fields: each field in turn takes the
+// candidate value with the smallest measured time (the others fixed), until a
+// full pass changes nothing (at most `passes` passes).  `measure` installs a
+// schedule, runs the timed solves and returns the mean milliseconds (< 0 if
+// the schedule failed).
+template <typename M>
+int tune_search(hodlr_schedule &best, double &best_ms, int precision,
+                const std::vector<int> &nb_opts, M &&measure, hodlr_tune_trial *log, int log_cap,
+                int *n_log) {
+  int nlog = 0;
+  auto record = [&](const hodlr_schedule &c, double ms) {
+    if (log && nlog < log_cap) log[nlog] = hodlr_tune_trial{c, ms};
+    ++nlog;
+  };
+  best_ms = measure(best);
+  record(best, best_ms);
+  if (!(best_ms >= 0)) return HODLR_ERR_CUDA;
+  const std::vector<int> rows = {256, 512, 1024, 2048};
+  const std::vector<int> ob32 = {0, 128, 256};
+  const std::vector<int> ob64 = {0, 64, 128};
+  const int nfields = 4;
+  for (int pass = 0; pass < 2; ++pass) {
+    bool changed = false;
+    for (int f = 0; f < nfields; ++f) {
+      std::vector<int> opts;
+      if (f == 0) opts = precision == HODLR_PREC_MIXED ? ob32 : ob64;
+      else if (f == 1) opts = precision == HODLR_PREC_MIXED ? nb_opts : std::vector<int>{};
+      else opts = rows;
+      for (int v : opts) {
+        hodlr_schedule c = best;
+        int &field = f == 0 ? (precision == HODLR_PREC_MIXED ? c.leaf_ob32 : c.leaf_ob64)
+                     : f == 1 ? c.leaf_nb
+                     : f == 2 ? c.reduce_rows
+                              : c.bcast_rows;
+        if (field == v) continue;
+        field = v;
+        const double ms = measure(c);
+        record(c, ms);
+        if (ms >= 0 && ms < 0.98 * best_ms) {  // keep a change only for a clear gain
+          best = c;
+          best_ms = ms;
+          changed = true;
+        }
       }
-      ++it;
-      rr = S.relres_read(s);
     }
-    if (iters) *iters = it;
-    if (relres) *relres = rr;
-    return rr <= tol ? 0 : HODLR_ERR_NOCONV;
+    if (!changed) break;
+  }
+  if (n_log) *n_log = nlog;
+  return 0;
+}
+
+// mean milliseconds of `reps` calls of fn on stream s (after one untimed call)
+template <typename F>
+double time_calls(cudaStream_t s, int reps, F &&fn) {
+  if (fn() < 0) return -1.0;
+  cudaEvent_t e0, e1;
+  HODLR_CUDA_TRY(cudaEventCreate(&e0));
+  HODLR_CUDA_TRY(cudaEventCreate(&e1));
+  HODLR_CUDA_TRY(cudaEventRecord(e0, s));
+  int rc = 0;
+  for (int i = 0; i < reps && rc >= 0; ++i) rc = fn();
+  HODLR_CUDA_TRY(cudaEventRecord(e1, s));
+  HODLR_CUDA_TRY(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc < 0 ? -1.0 : (double)ms / reps;
+}
+
+std::vector<int> nb_options(int nmax) {
+  std::vector<int> v = {0};
+  if (nmax <= 512) v.push_back(32);  // the default is 64 there
+  return v;
+}
+
+// A private stream for tuning: the solves are captured as CUDA graphs only
+// on a non-default stream, and the timed configuration is the replayed one.
+struct TuneStream {
+  cudaStream_t s = nullptr;
+  TuneStream() {
+    HODLR_CUDA_TRY(cudaDeviceSynchronize());
+    HODLR_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  }
+  ~TuneStream() {
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int hodlr_autotune(hodlr_system h, int precision, double tol, int reps, hodlr_schedule *best,
+                   double *best_ms, hodlr_tune_trial *log, int log_cap, int *n_log) {
+  if (!h) return -1;
+  if (precision != HODLR_PREC_FP64 && precision != HODLR_PREC_MIXED) return -2;
+  if (!(tol >= 0.0)) return -3;
+  if (reps < 1) return -4;
+  if (log_cap < 0) return -7;
+  return guarded([&]() -> int {
+    System &S = h->sys;
+    TuneStream ts;
+    auto measure = [&](const hodlr_schedule &c) -> double {
+      if (schedule_check(S, c)) return -1.0;
+      schedule_apply(S, c);
+      return time_calls(ts.s, reps, [&]() -> int {
+        if (precision == HODLR_PREC_MIXED)
+          return refined_body(S, precision, tol, 10, nullptr, nullptr, ts.s);
+        S.ensure_fp64();
+        S.run_graph(S.g_fused64[0], ts.s, [&]() { S.run_fused64(0, ts.s); });
+        S.factored = HODLR_PREC_FP64;
+        S.factored_form = 0;
+        return S.check_info(ts.s) ? -1 : 0;
+      });
+    };
+    hodlr_schedule b = schedule_of(S);
+    double ms = 0.0;
+    int rc = tune_search(b, ms, precision, nb_options(S.nmax), measure, log, log_cap, n_log);
+    if (rc) return rc;
+    schedule_apply(S, b);
+    if (best) *best = b;
+    if (best_ms) *best_ms = ms;
+    return 0;
   });
 }
 
@@ -881,6 +1078,31 @@ int hodlr_batch_destroy(hodlr_batch batch) {
   return 0;
 }
 
+// The refined solve of every system of a batch on stream s.
+static int batch_body(Batch &B, double tol, int maxiter, int *iters, double *relres_max,
+                      double *relres, int *failed, cudaStream_t s) {
+  B.run_graph(B.g_factor, s, [&]() { B.run_factor(s); });
+  for (System *S : B.sys) {
+    S->factored = HODLR_PREC_MIXED;
+    S->factored_form = 0;
+  }
+  int info = B.check_info(s, failed);
+  if (info) return info;
+  std::vector<double> per;
+  int it = 0;
+  double rr = B.relres_read(s, &per);
+  while (rr > tol && it < maxiter) {
+    B.run_graph(B.g_sweep, s, [&]() { B.run_sweep(s); });
+    ++it;
+    rr = B.relres_read(s, &per);
+  }
+  if (iters) *iters = it;
+  if (relres_max) *relres_max = rr;
+  if (relres)
+    for (size_t k = 0; k < per.size(); ++k) relres[k] = per[k];
+  return rr <= tol ? 0 : HODLR_ERR_NOCONV;
+}
+
 int hodlr_batch_solve_refined(hodlr_batch batch, double tol, int maxiter, int *iters,
                               double *relres_max, double *relres, int *failed,
                               hodlr_stream_t stream) {
@@ -888,28 +1110,41 @@ int hodlr_batch_solve_refined(hodlr_batch batch, double tol, int maxiter, int *i
   if (!(tol >= 0.0)) return -2;
   if (maxiter < 0) return -3;
   return guarded([&]() -> int {
+    return batch_body(batch->b, tol, maxiter, iters, relres_max, relres, failed,
+                      as_stream(stream));
+  });
+}
+
+int hodlr_batch_autotune(hodlr_batch batch, double tol, int reps, hodlr_schedule *best,
+                         double *best_ms, hodlr_tune_trial *log, int log_cap, int *n_log) {
+  if (!batch) return -1;
+  if (!(tol >= 0.0)) return -2;
+  if (reps < 1) return -3;
+  if (log_cap < 0) return -6;
+  return guarded([&]() -> int {
     Batch &B = batch->b;
-    cudaStream_t s = as_stream(stream);
-    B.run_graph(B.g_factor, s, [&]() { B.run_factor(s); });
-    for (System *S : B.sys) {
-      S->factored = HODLR_PREC_MIXED;
-      S->factored_form = 0;
-    }
-    int info = B.check_info(s, failed);
-    if (info) return info;
-    std::vector<double> per;
-    int it = 0;
-    double rr = B.relres_read(s, &per);
-    while (rr > tol && it < maxiter) {
-      B.run_graph(B.g_sweep, s, [&]() { B.run_sweep(s); });
-      ++it;
-      rr = B.relres_read(s, &per);
-    }
-    if (iters) *iters = it;
-    if (relres_max) *relres_max = rr;
-    if (relres)
-      for (size_t k = 0; k < per.size(); ++k) relres[k] = per[k];
-    return rr <= tol ? 0 : HODLR_ERR_NOCONV;
+    TuneStream ts;
+    int nmax = 0;
+    for (System *S : B.sys) nmax = std::max(nmax, S->nmax);
+    auto measure = [&](const hodlr_schedule &c) -> double {
+      for (System *S : B.sys)
+        if (schedule_check(*S, c)) return -1.0;
+      for (System *S : B.sys) schedule_apply(*S, c);
+      B.build(B.sys);
+      return time_calls(ts.s, reps, [&]() -> int {
+        const int rc = batch_body(B, tol, 10, nullptr, nullptr, nullptr, nullptr, ts.s);
+        return rc > 0 ? -1 : 0;
+      });
+    };
+    hodlr_schedule b = schedule_of(*B.sys[0]);
+    double ms = 0.0;
+    int rc = tune_search(b, ms, HODLR_PREC_MIXED, nb_options(nmax), measure, log, log_cap, n_log);
+    if (rc) return rc;
+    for (System *S : B.sys) schedule_apply(*S, b);
+    B.build(B.sys);
+    if (best) *best = b;
+    if (best_ms) *best_ms = ms;
+    return 0;
   });
 }
 

@@ -192,6 +192,27 @@ class HodlrMatrix:
         call("hodlr_relres", self.handle, ctypes.byref(out), _stream_ptr(stream))
         return out.value
 
+    # -- launch schedule -------------------------------------------------------
+    @property
+    def schedule(self) -> dict:
+        """The launch schedule (hodlr_schedule fields)."""
+        c = _lib.Schedule()
+        call("hodlr_get_schedule", self.handle, ctypes.byref(c))
+        return c.as_dict()
+
+    @schedule.setter
+    def schedule(self, d: dict):
+        cur = self.schedule
+        cur.update(d)
+        c = _lib.Schedule.from_dict(cur)
+        call("hodlr_set_schedule", self.handle, ctypes.byref(c))
+
+    def autotune(self, precision: int = PREC_MIXED, tol: float = 1e-12, reps: int = 2):
+        """Time candidate schedules on the current matrix and RHS and keep the
+        fastest; returns (schedule, ms per solve, [(schedule, ms), ...])."""
+        return _tune(lambda *a: lib.hodlr_autotune(self.handle, int(precision), *a),
+                     "hodlr_autotune", tol, reps)
+
     # -- per-phase device time ------------------------------------------------
     def set_profiling(self, on: bool):
         call("hodlr_set_profiling", self.handle, int(bool(on)))
@@ -277,6 +298,17 @@ class FastSolver:
         return it.value, rr.value
 
 
+def _tune(fn, name, tol, reps, cap=64):
+    best = _lib.Schedule()
+    ms = ctypes.c_double()
+    log = (_lib.TuneTrial * cap)()
+    n = ctypes.c_int()
+    check(name, fn(float(tol), int(reps), ctypes.byref(best), ctypes.byref(ms), log, cap,
+                   ctypes.byref(n)))
+    trials = [(log[i].schedule.as_dict(), log[i].ms) for i in range(min(n.value, cap))]
+    return best.as_dict(), ms.value, trials
+
+
 class SystemBatch:
     """Independent HODLR systems of uneven size, rank, leaf size and RHS count
     solved together (one merged launch per tree level and phase).  The
@@ -303,6 +335,12 @@ class SystemBatch:
         if check_conv or st != _lib.ERR_NOCONV:
             check("hodlr_batch_solve_refined", st)
         return it.value, list(rr)
+
+    def autotune(self, tol: float = 1e-12, reps: int = 2):
+        """One schedule for all systems, timed as the batched solve; returns
+        (schedule, ms per batched solve, [(schedule, ms), ...])."""
+        return _tune(lambda *a: lib.hodlr_batch_autotune(self._h, *a), "hodlr_batch_autotune",
+                     tol, reps)
 
     def set_profiling(self, on: bool):
         call("hodlr_batch_set_profiling", self._h, int(bool(on)))

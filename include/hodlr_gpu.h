@@ -281,6 +281,56 @@ int hodlr_batch_solve_refined(hodlr_batch batch, double tol, int maxiter, int *i
 int hodlr_batch_set_profiling(hodlr_batch batch, int on);
 int hodlr_batch_phase_times(hodlr_batch batch, double *ms, long long *launches, int reset);
 
+/* ---- Launch schedule and autotuner (no reference counterpart: the
+ * reference's task granularity is fixed by its tree).  A schedule fixes how
+ * the solve is cut into launches:
+ *   leaf_nb      FP32 leaf panel width: 0 = by the largest leaf (64 up to 512
+ *                rows, else 32), or 32, or 64 (leaves of <= 512 rows only);
+ *   leaf_ob32    FP32 leaf outer block width (a multiple of the panel width,
+ *                rounded down; 0 = one-level blocking);
+ *   leaf_ob64    the same for the FP64 path (panel width 32, or 16 above 512
+ *                rows);
+ *   reduce_rows  rows per split-K slot of the reduce V^T [d | u] (16..65536,
+ *                a multiple of 16; at most 64 slots per child);
+ *   bcast_rows   rows per item of the broadcast d -= u eta (16..65536, a
+ *                multiple of 16).
+ * Defaults: {0, 128, 0, 512, 512}.  Setting a schedule discards the system's
+ * factors (factor again before hodlr_solve); results are identical up to
+ * floating-point summation order. */
+typedef struct {
+  int leaf_nb;
+  int leaf_ob32;
+  int leaf_ob64;
+  int reduce_rows;
+  int bcast_rows;
+} hodlr_schedule;
+
+typedef struct {
+  hodlr_schedule schedule;
+  double ms; /* mean time of one timed solve; < 0: the schedule failed */
+} hodlr_tune_trial;
+
+int hodlr_get_schedule(hodlr_system sys, hodlr_schedule *out);
+int hodlr_set_schedule(hodlr_system sys, const hodlr_schedule *in);
+
+/* Autotuner: times candidate schedules on the system's current matrix and
+ * RHS with CUDA events (one untimed solve, then `reps` timed ones, each a
+ * full solve: precision MIXED = the refined solve to `tol`, FP64 = the fused
+ * FP64 solve), searching one field at a time (outer block, panel width,
+ * reduce rows, broadcast rows) from the current schedule, and installs the
+ * fastest.  Runs on a private stream after a device synchronization.  The
+ * system is left with the best schedule; its solution is the last trial's
+ * (solve again for the factors of the chosen schedule).  best, best_ms, log
+ * (log_cap entries) and n_log (trials run, may exceed log_cap) may be NULL. */
+int hodlr_autotune(hodlr_system sys, int precision, double tol, int reps,
+                   hodlr_schedule *best, double *best_ms, hodlr_tune_trial *log,
+                   int log_cap, int *n_log);
+/* The same for a batch (mixed precision): one schedule for all its systems,
+ * timed as the batched solve; the batch's merged plans are rebuilt. */
+int hodlr_batch_autotune(hodlr_batch batch, double tol, int reps, hodlr_schedule *best,
+                         double *best_ms, hodlr_tune_trial *log, int log_cap,
+                         int *n_log);
+
 /* Number of kernels this library launched on this thread since the last
  * reset (every launch from a hodlr_* call is counted). */
 long long hodlr_launch_count(void);

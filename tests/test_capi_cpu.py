@@ -65,6 +65,17 @@ def test_argument_errors_are_reported_before_device_use(fs):
     assert h.value is None
     assert lib.hodlr_batch_solve_refined(None, 1e-12, 10, None, None, None, None, None) == -1
     assert lib.hodlr_batch_destroy(None) == -1
+    assert lib.hodlr_get_schedule(None, None) == -1
+    assert lib.hodlr_set_schedule(None, None) == -1
+    assert lib.hodlr_autotune(None, 1, 1e-12, 2, None, None, None, 0, None) == -1
+    assert lib.hodlr_batch_autotune(None, 1e-12, 2, None, None, None, 0, None) == -1
+
+
+def test_schedule_cache_key(fs):
+    from fastsolver_b200 import autotune
+    h = fs.HodlrMatrix(16, 262144, 64, 512)
+    assert autotune.shape_key(h, fs.PREC_MIXED) == "N=262144,m=16,r=64,t=512,p=1"
+    assert autotune.load("/nonexistent/cache.json") == {}
 
 
 @pytest.mark.skipif(cuda_available(), reason="checks the no-device status")
