@@ -97,24 +97,34 @@ def phase_bytes(tree: np.ndarray, m: int, word: int):
     return b
 
 
-def leaf_update_bytes(tree: np.ndarray, word: int, nb: int = 64) -> float:
-    """Algorithmic bytes of all leaf trailing-update GEMMs of one factor pass:
-    per panel, C = A22|X (rest x (rest + ncols)) read and written, L21
-    (rest x kb) and U12 (kb x (rest + ncols)) read once."""
+def leaf_update_bytes(tree: np.ndarray, word: int, nb: int = 64, ob: int = 0) -> float:
+    """Algorithmic bytes of all leaf trailing-update GEMMs (C -= A B) of one
+    factor pass of the two-level blocked LU (outer blocks of `ob` columns,
+    panels of `nb`; ob <= nb is one level): per update item, C read and
+    written, A and B read once.  The items are those the library builds:
+    inside each block (rows below the panel x the block's columns right of
+    it), on the block rows (x the columns right of the block | X), and the
+    depth-ob trailing update (rows below the block x the same columns)."""
     nrow, ncol, rb, cb, lc, rc, par, dep, vnc, leaf = (tree[:, i] for i in range(10))
+    ob = ob // nb * nb if ob >= nb else nb
     tot = 0.0
+
+    def item(M, N, K):
+        return word * (2.0 * M * N + M * K + K * N) if M > 0 and N > 0 and K > 0 else 0.0
+
     for i in range(tree.shape[0]):
         if not leaf[i]:
             continue
         n = int(nrow[i])
         ncols = int(cb[i] + ncol[i])
-        for k0 in range(0, n, nb):
-            kb = min(nb, n - k0)
-            rest = n - k0 - kb
-            if rest <= 0:
-                continue
-            w = rest + ncols
-            tot += word * (2.0 * rest * w + rest * kb + kb * w)
+        for j0 in range(0, n, ob):
+            obe = min(ob, n - j0)
+            R = n - j0 - obe + ncols
+            for k0 in range(j0, j0 + obe, nb):
+                kb = min(nb, n - k0)
+                tot += item(n - k0 - kb, j0 + obe - k0 - kb, kb)   # inside the block
+                tot += item(j0 + obe - k0 - kb, R, kb)             # block rows
+            tot += item(n - j0 - obe, R, obe)                      # trailing, depth ob
     return tot
 
 
@@ -271,8 +281,22 @@ def run_batch(args):
     batch = fs.SystemBatch(hs)
     solver = fs.FastSolver()
 
+    # profiling runs launch eagerly on the legacy default stream (no CUDA
+    # graphs), so that the profiler sees ordinary kernel launches
+    run_stream = None if args.profile_one else stream
+
     def batch_step():
-        return batch.solve_refined(tol=TOL, maxiter=10, stream=stream)
+        return batch.solve_refined(tol=TOL, maxiter=10, stream=run_stream)
+
+    tune_info = None
+    if args.schedule:
+        for h in hs:
+            h.schedule = json.loads(args.schedule)
+        batch.close()
+        batch = fs.SystemBatch(hs)
+    elif not args.no_tune and not args.profile_one:
+        best, ms, trials = batch.autotune(tol=TOL, reps=1)
+        tune_info = {"schedule": best, "ms": round(ms, 4), "trials": len(trials)}
 
     if args.profile_one:
         for _ in range(2):
@@ -348,6 +372,7 @@ def run_batch(args):
             "batched_over_sequential_mixed": ms_seq / ms_batch,
             "batched_over_sequential_fp64": ms_fp64 / ms_batch,
             "phases_ms": {k: round(v[0], 4) for k, v in ph.items()},
+            "schedule": hs[0].schedule, "autotune": tune_info,
             "gpu_launches": int(launches), "clocks": clk,
             "e2e": None, "cpu_baseline": None,
         }
@@ -410,6 +435,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-solves", type=int, default=2)
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch schedule (skip the autotuner)")
+    ap.add_argument("--schedule", default=None,
+                    help="JSON launch schedule for every path (skips the autotuner), e.g. "
+                         "'{\"leaf_ob32\": 256}'")
     ap.add_argument("--profile-one", choices=["mixed", "fp64", "batch"], default=None,
                     help="warm up, then run one solve between cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off); prints no bench line")
@@ -450,13 +480,32 @@ def main():
     h = make_system(fs, cfg, args.seed + rank)
     tree = h.tree_nodes()
     solver = fs.FastSolver()
+    # launch schedules from the autotuner (untimed): one per path, installed
+    # before that path's warm-up
+    if args.schedule:
+        h.schedule = json.loads(args.schedule)
+    sched_default = h.schedule
+    sched = {"mixed": sched_default, "fp64": sched_default}
+    tune_info = None
+    if not args.no_tune and not args.profile_one and not args.schedule:
+        tune_info = {}
+        for name, prec in (("mixed", fs.PREC_MIXED), ("fp64", fs.PREC_FP64)):
+            h.schedule = sched_default
+            best, ms, trials = h.autotune(prec, tol=TOL, reps=2)
+            sched[name] = best
+            tune_info[name] = {"schedule": best, "ms": round(ms, 4), "trials": len(trials)}
+    h.schedule = sched["mixed"]
+
+    # profiling runs launch eagerly on the legacy default stream (no CUDA
+    # graphs), so that the profiler sees ordinary kernel launches
+    run_stream = None if args.profile_one else stream
 
     def mixed_step():
-        it, rr = solver.solve_refined(h, fs.PREC_MIXED, tol=TOL, maxiter=10, stream=stream)
+        it, rr = solver.solve_refined(h, fs.PREC_MIXED, tol=TOL, maxiter=10, stream=run_stream)
         return it, rr
 
     def fp64_step():
-        solver.bfs_solve(h, sync=False, stream=stream)
+        solver.bfs_solve(h, sync=False, stream=run_stream)
 
     if args.profile_one:
         step = mixed_step if args.profile_one == "mixed" else fp64_step
@@ -496,6 +545,7 @@ def main():
     barrier()
 
     # ---- timed: plain FP64 path
+    h.schedule = sched["fp64"]
     for _ in range(args.warmup):
         fp64_step()
     torch.cuda.synchronize()
@@ -508,13 +558,14 @@ def main():
     ms_fp64 = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     rr_fp64 = h.relres(stream=stream)
 
-    # ---- per-phase device time (separate, event-bracketed pass)
+    # ---- per-phase device time (separate, event-bracketed passes)
     h.set_profiling(True)
-    mixed_step()
-    ph_mixed = h.phase_times(reset=True)
     fp64_step()
     torch.cuda.synchronize()
     ph_fp64 = h.phase_times(reset=True)
+    h.schedule = sched["mixed"]
+    mixed_step()
+    ph_mixed = h.phase_times(reset=True)
     h.set_profiling(False)
 
     # ---- end to end through the public API from pinned host memory
@@ -574,7 +625,9 @@ def main():
     ph_f = h.phase_times(reset=True)
     h.set_profiling(False)
     ms_upd, n_upd = ph_f["leaf_update"]
-    upd_bytes = leaf_update_bytes(tree, 4)
+    sm = sched["mixed"]
+    nb_used = sm["leaf_nb"] or (64 if int(tree[tree[:, 9] == 1, 0].max()) <= 512 else 32)
+    upd_bytes = leaf_update_bytes(tree, 4, nb_used, sm["leaf_ob32"])
     per_launch_ms = ms_upd / max(n_upd, 1)
     bytes_per_launch = upd_bytes / max(n_upd, 1)
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
@@ -637,6 +690,7 @@ def main():
                       "fp64": {k: round(v[0], 4) for k, v in ph_fp64.items()}},
         "peaks": {"hbm_gbs": pk["hbm"], "src": pk["src"], "fp64_tflops_nominal": fp64_peak,
                   "fp32_tflops_nominal": fp32_peak},
+        "schedules": {"mixed": sched["mixed"], "fp64": sched["fp64"], "autotune": tune_info},
         "gpu_launches": int(launches),
         "clocks": clk,
         "e2e": e2e,

@@ -77,6 +77,69 @@ struct Vec {
   static constexpr int W = 16 / sizeof(T);
 };
 
+// ---------------------------------------------------------------- NN (rows)
+// FP32 C (M x N <= NC) = beta Cin + alpha sum_s A_s B_s with one row per
+// thread: A is read straight from global memory (a warp reads 32 consecutive
+// rows of one column: 128 bytes), 32 (16 when NC = 32) k-values in flight
+// per thread, while the matching block of B sits in shared memory.  Small CTAs (128 rows)
+// and no A staging let many CTAs share an SM, which keeps enough loads in
+// flight for the short-K products of the refinement sweeps (K = r).
+constexpr int kRowThreads = 128;
+
+template <int NC>
+__global__ void __launch_bounds__(kRowThreads)
+    skinny_nn_rows_kernel(const GemmItem<float, float> *__restrict__ items,
+                          const GemmSeg<float> *__restrict__ segs, float alpha, float beta) {
+  constexpr int kRowKC = NC > 16 ? 16 : 32;  // k-values in flight per thread
+  __shared__ __align__(16) float Bs[kRowKC * NC];
+  const GemmItem<float, float> it = items[blockIdx.x];
+  const int row0 = blockIdx.y * kRowThreads;
+  if (row0 >= it.M) return;
+  const int tid = threadIdx.x;
+  const int row = row0 + tid;
+  const bool live = row < it.M;
+  const int N = it.N;
+  float acc[NC];
+#pragma unroll
+  for (int n = 0; n < NC; ++n) acc[n] = 0.f;
+  for (int sidx = it.seg_begin; sidx < it.seg_begin + it.seg_count; ++sidx) {
+    const GemmSeg<float> sg = segs[sidx];
+    for (int k0 = 0; k0 < sg.K; k0 += kRowKC) {
+      const int kc = min(kRowKC, sg.K - k0);
+      // this chunk's A values of the thread's row (issued before the barrier)
+      float a[kRowKC];
+      const float *ap = sg.A + (live ? row : 0) + (long long)k0 * sg.lda;
+#pragma unroll
+      for (int k = 0; k < kRowKC; ++k) a[k] = (k < kc) ? __ldg(ap + (long long)k * sg.lda) : 0.f;
+      __syncthreads();  // the previous chunk's B reads are done
+      for (int e = tid; e < kRowKC * NC; e += kRowThreads) {
+        const int k = e % kRowKC, n = e / kRowKC;
+        Bs[k * NC + n] = (k < kc && n < N) ? __ldg(sg.B + (k0 + k) + (long long)n * sg.ldb) : 0.f;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kRowKC; ++k) {
+#pragma unroll
+        for (int n = 0; n < NC; n += 4) {
+          const float4 b = *reinterpret_cast<const float4 *>(Bs + k * NC + n);
+          acc[n] += a[k] * b.x;
+          acc[n + 1] += a[k] * b.y;
+          acc[n + 2] += a[k] * b.z;
+          acc[n + 3] += a[k] * b.w;
+        }
+      }
+    }
+  }
+  if (!live) return;
+#pragma unroll
+  for (int n = 0; n < NC; ++n) {
+    if (n >= N) break;
+    float v = alpha * acc[n];
+    if (it.Cin) v += beta * it.Cin[row + (long long)n * it.ldcin];
+    it.C[row + (long long)n * it.ldc] = v;
+  }
+}
+
 // ---------------------------------------------------------------- NN
 // CTA = 512 rows of one item, thread = rows (r, r + 256), 2 x NC accumulators,
 // so every broadcast read of B feeds two rows.
@@ -568,6 +631,13 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid(nitems, cdiv(max_m, TM), cdiv(max_n, TN));
     skinny_tn2_kernel<T><<<grid, kTNThreads, smem, s>>>(items, segs, alpha, beta);
+  } else if constexpr (sizeof(T) == 4) {
+    dim3 grid(nitems, cdiv(max_m, kRowThreads));
+    const auto *fi = reinterpret_cast<const GemmItem<float, float> *>(items);
+    const auto *fs = reinterpret_cast<const GemmSeg<float> *>(segs);
+    if (max_n <= 8) skinny_nn_rows_kernel<8><<<grid, kRowThreads, 0, s>>>(fi, fs, alpha, beta);
+    else if (max_n <= 16) skinny_nn_rows_kernel<16><<<grid, kRowThreads, 0, s>>>(fi, fs, alpha, beta);
+    else skinny_nn_rows_kernel<32><<<grid, kRowThreads, 0, s>>>(fi, fs, alpha, beta);
   } else {
     constexpr int KT = nn_kt<T>();
     dim3 grid(nitems, cdiv(max_m, kNNRows));

@@ -14,26 +14,86 @@ inline int grid_for(long long n) {
   return (int)(b > 0 ? b : 1);
 }
 
-template <typename TS, typename TD>
-__global__ void convert2d_kernel(const TS *__restrict__ src, long long lds, TD *__restrict__ dst,
-                                 long long ldd, long long rows, long long cols) {
-  const long long total = rows * cols;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long i = e % rows, j = e / rows;
-    dst[i + j * ldd] = TD(src[i + j * lds]);
+// 4 consecutive rows of one column: dst = TD(src) or dst += TD(src); 16-byte
+// vector accesses when `vec` (both column starts 16-byte aligned and all 4
+// rows inside the matrix), else element by element.
+template <typename T>
+struct Vec4 {
+  T v[4];
+};
+template <typename T>
+__device__ inline Vec4<T> load4(const T *p) {
+  Vec4<T> r;
+  if constexpr (sizeof(T) == 4) {
+    const float4 x = *reinterpret_cast<const float4 *>(p);
+    r.v[0] = x.x; r.v[1] = x.y; r.v[2] = x.z; r.v[3] = x.w;
+  } else {
+    const double2 x = reinterpret_cast<const double2 *>(p)[0];
+    const double2 y = reinterpret_cast<const double2 *>(p)[1];
+    r.v[0] = x.x; r.v[1] = x.y; r.v[2] = y.x; r.v[3] = y.y;
+  }
+  return r;
+}
+template <typename T>
+__device__ inline void store4(T *p, const Vec4<T> &r) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+  } else {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(r.v[0], r.v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(r.v[2], r.v[3]);
+  }
+}
+template <typename TS, typename TD, bool ADD>
+__device__ inline void move4(const TS *__restrict__ src, TD *__restrict__ dst, long long i,
+                             long long rows, bool vec) {
+  if (vec && i + 4 <= rows) {
+    const Vec4<TS> x = load4(src + i);
+    Vec4<TD> y;
+    if (ADD) y = load4(dst + i);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) y.v[u] = ADD ? TD(y.v[u] + TD(x.v[u])) : TD(x.v[u]);
+    store4(dst + i, y);
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (i + u < rows) {
+        if (ADD) dst[i + u] += TD(src[i + u]);
+        else dst[i + u] = TD(src[i + u]);
+      }
   }
 }
 
-template <typename TS>
-__global__ void add2d_kernel(double *__restrict__ x, long long ldx, const TS *__restrict__ y,
-                             long long ldy, long long rows, long long cols) {
-  const long long total = rows * cols;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long i = e % rows, j = e / rows;
-    x[i + j * ldx] += double(y[i + j * ldy]);
+constexpr int kTileRows = 4 * kThreads;  // rows of one (column, tile) work unit
+
+// dst (rows x cols, ldd) = TD(src) (or += with ADD): a grid-stride loop over
+// (column, kTileRows-row tile) units, each thread moving 4 consecutive rows.
+template <typename TS, typename TD, bool ADD>
+__global__ void ew_tile_kernel(const TS *__restrict__ src, long long lds, TD *__restrict__ dst,
+                               long long ldd, long long rows, long long cols, bool vec) {
+  const long long rtiles = cdiv<long long>(rows, kTileRows);
+  const long long total = rtiles * cols;
+  for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+    const long long j = t / rtiles;
+    const long long i = (t - j * rtiles) * kTileRows + 4 * threadIdx.x;
+    move4<TS, TD, ADD>(src + j * lds, dst + j * ldd, i, rows, vec);
   }
+}
+
+template <typename TS, typename TD>
+bool vec_ok(const TS *src, long long lds, const TD *dst, long long ldd) {
+  return (reinterpret_cast<uintptr_t>(src) % 16 == 0) && (reinterpret_cast<uintptr_t>(dst) % 16 == 0) &&
+         (lds * (long long)sizeof(TS)) % 16 == 0 && (ldd * (long long)sizeof(TD)) % 16 == 0;
+}
+
+template <typename TS, typename TD, bool ADD>
+void launch_ew_tile(const TS *src, long long lds, TD *dst, long long ldd, long long rows,
+                    long long cols, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  const long long units = cdiv<long long>(rows, kTileRows) * cols;
+  const unsigned grid = (unsigned)std::min<long long>(units, 148LL * 8);
+  ew_tile_kernel<TS, TD, ADD><<<grid, kThreads, 0, s>>>(src, lds, dst, ldd, rows, cols,
+                                                         vec_ok(src, lds, dst, ldd));
+  HODLR_LAUNCH_CHECK();
 }
 
 // out[c] = sqrt(sum_i r(i,c)^2) / sqrt(sum_i b(i,c)^2), one CTA per column.
@@ -80,17 +140,12 @@ __global__ void ew2d_batched_kernel(const Ew2DTask<TS, TD> *__restrict__ tasks, 
     const long long lt = t - tk.tile0;
     const long long j = lt / rtiles;
     const long long i0 = (lt - j * rtiles) * kEwTileRows;
-    const TS *src = tk.src + j * tk.lds;
-    TD *dst = tk.dst + j * tk.ldd;
-    const long long rows = tk.rows;
-#pragma unroll
-    for (int q = 0; q < kEwTileRows / kThreads; ++q) {
-      const long long i = i0 + q * kThreads + threadIdx.x;
-      if (i < rows) {
-        if (ADD) dst[i] += TD(src[i]);
-        else dst[i] = TD(src[i]);
-      }
-    }
+    const bool vec = (reinterpret_cast<uintptr_t>(tk.src) % 16 == 0) &&
+                     (reinterpret_cast<uintptr_t>(tk.dst) % 16 == 0) &&
+                     (tk.lds * (long long)sizeof(TS)) % 16 == 0 &&
+                     (tk.ldd * (long long)sizeof(TD)) % 16 == 0;
+    move4<TS, TD, ADD>(tk.src + j * tk.lds, tk.dst + j * tk.ldd, i0 + 4 * threadIdx.x, tk.rows,
+                       vec);
   }
 }
 
@@ -302,10 +357,7 @@ void launch_scale_batched(const FillTask *tasks, int ntasks, long long max_elems
 template <typename TS, typename TD>
 void launch_convert2d(const TS *src, long long lds, TD *dst, long long ldd, long long rows,
                       long long cols, cudaStream_t s) {
-  if (rows <= 0 || cols <= 0) return;
-  convert2d_kernel<TS, TD><<<grid_for(rows * cols), kThreads, 0, s>>>(src, lds, dst, ldd, rows,
-                                                                       cols);
-  HODLR_LAUNCH_CHECK();
+  launch_ew_tile<TS, TD, false>(src, lds, dst, ldd, rows, cols, s);
 }
 template void launch_convert2d<double, float>(const double *, long long, float *, long long,
                                               long long, long long, cudaStream_t);
@@ -317,9 +369,7 @@ template void launch_convert2d<double, double>(const double *, long long, double
 template <typename TS>
 void launch_add2d(double *x, long long ldx, const TS *y, long long ldy, long long rows,
                   long long cols, cudaStream_t s) {
-  if (rows <= 0 || cols <= 0) return;
-  add2d_kernel<TS><<<grid_for(rows * cols), kThreads, 0, s>>>(x, ldx, y, ldy, rows, cols);
-  HODLR_LAUNCH_CHECK();
+  launch_ew_tile<TS, double, true>(y, ldy, x, ldx, rows, cols, s);
 }
 template void launch_add2d<float>(double *, long long, const float *, long long, long long,
                                   long long, cudaStream_t);
