@@ -1,0 +1,103 @@
+"""Host-side logic that needs no GPU: the schedule cache over the autotuner,
+the benchmark's algorithmic-bytes model of the two-level leaf LU, and the
+batched workload's seeded draw."""
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+
+class FakeMatrix:
+    """Stands in for HodlrMatrix: a schedule property and a counting tuner."""
+
+    def __init__(self, N=4096, m=2, r=16, t=256):
+        self.rhs_rows, self.rhs_cols, self.rank, self.threshold = N, m, r, t
+        self._sched = {"leaf_nb": 0, "leaf_ob32": 128, "leaf_ob64": 0, "reduce_rows": 512,
+                       "bcast_rows": 512}
+        self.tuned = 0
+
+    @property
+    def schedule(self):
+        return dict(self._sched)
+
+    @schedule.setter
+    def schedule(self, d):
+        self._sched.update(d)
+
+    def autotune(self, precision, tol=1e-12, reps=2):
+        self.tuned += 1
+        best = dict(self._sched, bcast_rows=1024)
+        self._sched = best
+        return best, 1.5, [(best, 1.5)] * 7
+
+
+def test_schedule_cache_tunes_once_per_shape(tmp_path):
+    from fastsolver_b200 import autotune
+    cache = str(tmp_path / "sched.json")
+    a = FakeMatrix()
+    s1 = autotune.tuned(a, 1, cache=cache)
+    assert a.tuned == 1 and s1["bcast_rows"] == 1024
+    table = json.load(open(cache))
+    assert list(table) == ["N=4096,m=2,r=16,t=256,p=1"]
+    b = FakeMatrix()                       # same shape: installed from the cache
+    assert autotune.tuned(b, 1, cache=cache) == s1
+    assert b.tuned == 0 and b.schedule["bcast_rows"] == 1024
+    c = FakeMatrix(N=8192)                 # another shape: tuned and added
+    autotune.tuned(c, 1, cache=cache)
+    assert c.tuned == 1 and len(json.load(open(cache))) == 2
+    d = FakeMatrix()                       # another precision: its own entry
+    autotune.tuned(d, 0, cache=cache)
+    assert d.tuned == 1 and len(json.load(open(cache))) == 3
+
+
+def _one_level_bytes(tree, word, nb):
+    """The one-level right-looking LU's update bytes, written out directly."""
+    tot = 0.0
+    for i in range(tree.shape[0]):
+        if not tree[i, 9]:
+            continue
+        n, ncols = int(tree[i, 0]), int(tree[i, 3] + tree[i, 1])
+        for k0 in range(0, n, nb):
+            kb = min(nb, n - k0)
+            rest = n - k0 - kb
+            if rest > 0:
+                w = rest + ncols
+                tot += word * (2.0 * rest * w + rest * kb + kb * w)
+    return tot
+
+
+@pytest.mark.parametrize("N,m,r,t", [(262144, 16, 64, 512), (9001, 3, 40, 1024),
+                                     (3001, 5, 12, 200)])
+def test_leaf_update_bytes_model(fs, N, m, r, t):
+    import bench
+    tree = fs.build_tree(N, m, r, t)
+    for nb in (32, 64):
+        one = bench.leaf_update_bytes(tree, 4, nb, 0)
+        assert one == pytest.approx(_one_level_bytes(tree, 4, nb), rel=1e-12)
+        assert bench.leaf_update_bytes(tree, 4, nb, nb) == pytest.approx(one, rel=1e-12)
+        # deeper trailing updates pay off once a leaf spans several outer
+        # blocks (for small leaves the in-block work can cost more: the
+        # autotuner decides)
+        if int(tree[tree[:, 9] == 1, 0].max()) >= 4 * (4 * nb):
+            assert bench.leaf_update_bytes(tree, 4, nb, 4 * nb) < one
+    if (N, t) == (262144, 512):   # the benchmark system: 7.7 GB -> 5.4 GB per factorization
+        assert bench.leaf_update_bytes(tree, 4, 64, 0) == pytest.approx(7.707e9, rel=1e-3)
+        assert bench.leaf_update_bytes(tree, 4, 64, 128) == pytest.approx(5.373e9, rel=1e-3)
+
+
+def test_batch_draw_is_seeded_and_in_range():
+    import bench
+    a = bench.batch_systems(1245667)
+    assert a == bench.batch_systems(1245667) and a != bench.batch_systems(1)
+    assert len(a) == 64
+    Ns = np.array([c["N"] for c in a])
+    assert Ns.min() >= 8192 and Ns.max() <= 131072
+    assert {c["leaf"] for c in a} <= {256, 512, 1024} and len({c["leaf"] for c in a}) == 3
+    assert all(16 <= c["rank"] <= 96 and 1 <= c["nrhs"] <= 32 for c in a)
+    # log-uniform: the median sits near the geometric mean of the range
+    assert 20000 < np.median(Ns) < 50000
