@@ -21,6 +21,8 @@
 //                                      X[0:k0] -= U[0:k0, k] X[k]
 // so D ends as LAPACK's P L U factors, X as D^{-1} X.  The GEMMs are items of
 // the batched GEMM engine (gemm_simt.cu), one launch per step for all leaves.
+#include <algorithm>
+
 #include "common.cuh"
 #include "leaf_blocked.cuh"
 
@@ -286,6 +288,9 @@ __global__ void __launch_bounds__(kRegThreads, 1)
   const int kb = min(NB, n - k0);
   const int R = n - k0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // the launch gives one thread per row (RPT rows per thread) of the panel's
+  // live part, at most kRegThreads: later panels run with fewer warps
+  const int nthr = blockDim.x, nw = nthr >> 5;
   T *D = tk.D;
   const long long ldd = tk.ldd;
   T a[RPT][NB];
@@ -293,7 +298,7 @@ __global__ void __launch_bounds__(kRegThreads, 1)
   bool live[RPT];
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
-    const int i = tid + q * kRegThreads;
+    const int i = tid + q * nthr;
     live[q] = i < R;
     pos[q] = i;
     const T *src = D + (k0 + i) + (long long)k0 * ldd;
@@ -328,7 +333,7 @@ __global__ void __launch_bounds__(kRegThreads, 1)
               const T av = tabs(a[q][jj]);
               // NaN is never a candidate (as idamax, which skips it)
               if (av == av && (bp == 0x7fffffff || av > best || (av == best && pos[q] < bp))) {
-                best = av; bp = pos[q]; bc = tid + q * kRegThreads;
+                best = av; bp = pos[q]; bc = tid + q * nthr;
               }
             }
           }
@@ -337,7 +342,7 @@ __global__ void __launch_bounds__(kRegThreads, 1)
           // the winning lane publishes its row (rotated like every row)
 #pragma unroll
           for (int q = 0; q < RPT; ++q) {
-            if (bc >= 0 && bc == tid + q * kRegThreads) {
+            if (bc >= 0 && bc == tid + q * nthr) {
               V *dst = reinterpret_cast<V *>(wrow[slot][warp]);
 #pragma unroll
               for (int cv = 0; cv < NB / VW; ++cv) {
@@ -357,7 +362,7 @@ __global__ void __launch_bounds__(kRegThreads, 1)
         // combine the warp candidates (every thread, same result)
         T pb = T(0);
         int pp = 0x7fffffff, pc = -1, pw = 0;
-        if (lane < NW) { pb = wval[slot][lane]; pp = wpos[slot][lane]; pc = wcode[slot][lane]; }
+        if (lane < nw) { pb = wval[slot][lane]; pp = wpos[slot][lane]; pc = wcode[slot][lane]; }
         warp_argmax(pb, pp, pc, pw);  // pw: the winning warp
         int p = j;
         T piv = T(0);
@@ -368,7 +373,7 @@ __global__ void __launch_bounds__(kRegThreads, 1)
 #pragma unroll
           for (int q = 0; q < RPT; ++q) {
             if (live[q]) {
-              if (tid + q * kRegThreads == pc) pos[q] = j;
+              if (tid + q * nthr == pc) pos[q] = j;
               else if (pos[q] == j) pos[q] = p;
             }
           }
@@ -412,7 +417,7 @@ __global__ void __launch_bounds__(kRegThreads, 1)
   int pold[RPT];
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
-    pold[q] = live[q] ? tk.perm[k0 + tid + q * kRegThreads] : 0;
+    pold[q] = live[q] ? tk.perm[k0 + tid + q * nthr] : 0;
     if (live[q]) {
       T *dst = D + (k0 + pos[q]) + (long long)k0 * ldd;
 #pragma unroll
@@ -428,7 +433,7 @@ __global__ void __launch_bounds__(kRegThreads, 1)
       }
     }
   }
-  for (int r = kb + tid; r < NB; r += kRegThreads) {
+  for (int r = kb + tid; r < NB; r += nthr) {
     for (int c = 0; c < NB; ++c) {
       Lr[r * LDL + c] = c == r ? T(1) : T(0);
       Ur[r * LDL + c] = c == r ? T(1) : T(0);
@@ -438,8 +443,8 @@ __global__ void __launch_bounds__(kRegThreads, 1)
 #pragma unroll
   for (int q = 0; q < RPT; ++q)
     if (live[q]) tk.perm[k0 + pos[q]] = pold[q];
-  for (int j = tid; j < kb; j += kRegThreads) tk.ipiv[k0 + j] = k0 + pv[j] + 1;
-  for (int r = tid; r < NB; r += kRegThreads) udr[r] = T(1) / Ur[r * LDL + r];
+  for (int j = tid; j < kb; j += nthr) tk.ipiv[k0 + j] = k0 + pv[j] + 1;
+  for (int r = tid; r < NB; r += nthr) udr[r] = T(1) / Ur[r * LDL + r];
   if (tid == 0) {
     tk.swapflag[panel] = swaps ? 1 : 0;
     if (info_local && info && info[tk.info_slot] == 0) info[tk.info_slot] = info_local;
@@ -450,7 +455,7 @@ __global__ void __launch_bounds__(kRegThreads, 1)
   constexpr int RPL = (NB + 31) / 32;
   T *Lout = tk.Linv + (size_t)panel * NB * NB;
   T *Uout = tk.Uinv + (size_t)panel * NB * NB;
-  for (int j0 = warp * 4; j0 < NB; j0 += NW * 4) {
+  for (int j0 = warp * 4; j0 < NB; j0 += nw * 4) {
     T x[4][RPL];
     // L^{-1}: forward substitution on e_j
 #pragma unroll
@@ -773,9 +778,11 @@ void launch_leaf_panel_nb(const LeafFactorTask<T> *tasks, int count, int max_n, 
 }
 
 template <typename T, int NB, int RPT>
-void launch_leaf_panel_reg(const LeafFactorTask<T> *tasks, int count, int k0, int panel,
-                           int *info, cudaStream_t s) {
-  leaf_panel_reg_kernel<T, NB, RPT><<<count, kRegThreads, 0, s>>>(tasks, k0, panel, info);
+void launch_leaf_panel_reg(const LeafFactorTask<T> *tasks, int count, int rows, int k0,
+                           int panel, int *info, cudaStream_t s) {
+  // one warp per 32 x RPT live rows of the largest leaf's panel
+  const int threads = std::min(kRegThreads, std::max(32, cdiv(cdiv(rows, RPT), 32) * 32));
+  leaf_panel_reg_kernel<T, NB, RPT><<<count, threads, 0, s>>>(tasks, k0, panel, info);
   HODLR_LAUNCH_CHECK();
 }
 
@@ -787,14 +794,14 @@ void launch_leaf_panel(const LeafFactorTask<T> *tasks, int count, int max_n, int
   const int rows = max_n - k0;
   if constexpr (sizeof(T) == 4) {
     if (nb == 64 && rows <= kRegThreads)
-      return launch_leaf_panel_reg<T, 64, 1>(tasks, count, k0, panel, info, s);
+      return launch_leaf_panel_reg<T, 64, 1>(tasks, count, rows, k0, panel, info, s);
     if (nb == 32 && rows <= 2 * kRegThreads)
-      return launch_leaf_panel_reg<T, 32, 2>(tasks, count, k0, panel, info, s);
+      return launch_leaf_panel_reg<T, 32, 2>(tasks, count, rows, k0, panel, info, s);
   } else {
     if (nb == 32 && rows <= kRegThreads)
-      return launch_leaf_panel_reg<T, 32, 1>(tasks, count, k0, panel, info, s);
+      return launch_leaf_panel_reg<T, 32, 1>(tasks, count, rows, k0, panel, info, s);
     if (nb == 16 && rows <= 2 * kRegThreads)
-      return launch_leaf_panel_reg<T, 16, 2>(tasks, count, k0, panel, info, s);
+      return launch_leaf_panel_reg<T, 16, 2>(tasks, count, rows, k0, panel, info, s);
   }
   if (sizeof(T) == 8) {
     if (nb == 32) launch_leaf_panel_nb<T, 32>(tasks, count, max_n, k0, panel, info, s);
