@@ -103,10 +103,14 @@ def leaf_update_bytes(tree: np.ndarray, word: int, nb: int = 64, ob: int = 0) ->
     panels of `nb`; ob <= nb is one level): per update item, C read and
     written, A and B read once.  The items are those the library builds:
     inside each block (rows below the panel x the block's columns right of
-    it), on the block rows (x the columns right of the block | X), and the
-    depth-ob trailing update (rows below the block x the same columns)."""
+    it), on the block rows (x the columns right of the block | X) when those
+    are solved panel by panel (ob > 128), and the depth-ob trailing update
+    (rows below the block x the same columns).  With nb < ob <= 128 the block
+    rows are solved by one product with the block's triangular inverse (a
+    solve, not an update)."""
     nrow, ncol, rb, cb, lc, rc, par, dep, vnc, leaf = (tree[:, i] for i in range(10))
     ob = ob // nb * nb if ob >= nb else nb
+    binv = nb < ob <= 128
     tot = 0.0
 
     def item(M, N, K):
@@ -123,7 +127,8 @@ def leaf_update_bytes(tree: np.ndarray, word: int, nb: int = 64, ob: int = 0) ->
             for k0 in range(j0, j0 + obe, nb):
                 kb = min(nb, n - k0)
                 tot += item(n - k0 - kb, j0 + obe - k0 - kb, kb)   # inside the block
-                tot += item(j0 + obe - k0 - kb, R, kb)             # block rows
+                if not binv:
+                    tot += item(j0 + obe - k0 - kb, R, kb)         # block rows
             tot += item(n - j0 - obe, R, obe)                      # trailing, depth ob
     return tot
 

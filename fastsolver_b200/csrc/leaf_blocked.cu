@@ -749,6 +749,129 @@ __global__ void __launch_bounds__(kApplyThreads)
   }
 }
 
+// ---- inverses of the outer diagonal blocks (two-level factorization).
+//
+// For outer block J (rows / columns j0 .. j0 + obe of a leaf) with panels
+// p = 0 .. P-1 of width NB, the unit-lower block inverse is built by block
+// forward substitution from the panels' own inverses Linv_p:
+//   X[p][p] = Linv_p,  X[p][q] = -Linv_p sum_{s=q}^{p-1} L[p][s] X[s][q]  (q < p),
+// and the upper one by block back substitution from Uinv_p:
+//   Y[p][p] = Uinv_p,  Y[q][p] = -Uinv_q sum_{s=q+1}^{p} U[q][s] Y[s][p]  (q < p).
+// CTA (256 threads) = one leaf x {lower, upper}; the ob x ob result, an NB x NB
+// product tile and two staged NB x NB operands live in shared memory (padded
+// leading dimensions), products are 16 x 16 thread grids of R x R outputs.
+constexpr int kInvThreads = 256;
+
+template <typename T, int NB>
+__device__ inline void tile_mm(const T *A, int lda, const T *B, int ldb, T *C, int ldc,
+                               T alpha, bool acc) {
+  constexpr int R = NB / 16;
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+  T c[R][R];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int q = 0; q < R; ++q) c[r][q] = T(0);
+#pragma unroll 4
+  for (int k = 0; k < NB; ++k) {
+    T a[R], b[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) a[r] = A[(ty * R + r) + k * lda];
+#pragma unroll
+    for (int q = 0; q < R; ++q) b[q] = B[k + (tx * R + q) * ldb];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int q = 0; q < R; ++q) c[r][q] += a[r] * b[q];
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      T *cp = C + (ty * R + r) + (tx * R + q) * ldc;
+      *cp = (acc ? *cp : T(0)) + alpha * c[r][q];
+    }
+}
+
+template <typename T, int NB>
+__global__ void __launch_bounds__(kInvThreads)
+    leaf_block_inverse_kernel(const LeafFactorTask<T> *__restrict__ tasks, int ob, int J) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const LeafFactorTask<T> tk = tasks[blockIdx.x];
+  const int n = tk.n;
+  const int j0 = J * ob;
+  if (j0 >= n) return;
+  const int obe = min(ob, n - j0);
+  const int P = (obe + NB - 1) / NB;
+  const int pbase = j0 / NB;
+  const bool upper = blockIdx.y == 1;
+  constexpr int LT = NB + 1;  // padded ld of the NB x NB tiles
+  const int LX = ob + 1;      // padded ld of the block inverse
+  T *X = reinterpret_cast<T *>(smem_raw);  // ob x ob
+  T *Tt = X + (size_t)ob * LX;             // product tile
+  T *As = Tt + NB * LT;                    // staged panel inverse
+  T *Bs = As + NB * LT;                    // staged L / U block of D
+  const int tid = threadIdx.x;
+  for (int e = tid; e < ob * ob; e += kInvThreads) X[(e % ob) + (e / ob) * LX] = T(0);
+  // stage panel pi's inverse (NB x NB, ld NB; identity beyond the leaf)
+  auto stage_inv = [&](int pi) {
+    const T *src = (upper ? tk.Uinv : tk.Linv) + (size_t)pi * NB * NB;
+    for (int e = tid; e < NB * NB; e += kInvThreads) As[(e % NB) + (e / NB) * LT] = src[e];
+  };
+  // stage the NB x NB block of D at block panels (pr, pc), zero outside the block
+  auto stage_d = [&](int pr, int pc) {
+    for (int e = tid; e < NB * NB; e += kInvThreads) {
+      const int i = e % NB, c = e / NB;
+      const int gi = pr * NB + i, gc = pc * NB + c;
+      Bs[i + c * LT] = (gi < obe && gc < obe) ? tk.D[(j0 + gi) + (long long)(j0 + gc) * tk.ldd] : T(0);
+    }
+  };
+  auto Xb = [&](int pr, int pc) { return X + pr * NB + (size_t)pc * NB * LX; };
+  for (int p = 0; p < P; ++p) {
+    __syncthreads();
+    stage_inv(pbase + p);
+    __syncthreads();
+    for (int e = tid; e < NB * NB; e += kInvThreads) {
+      const int i = e % NB, c = e / NB;
+      if (p * NB + i < ob && p * NB + c < ob) Xb(p, p)[i + c * LX] = As[i + c * LT];
+    }
+    if (!upper) {
+      for (int q = 0; q < p; ++q) {
+        // Tt = sum_{s=q}^{p-1} L[p][s] X[s][q];  X[p][q] = -Linv_p Tt
+        for (int s2 = q; s2 < p; ++s2) {
+          __syncthreads();
+          stage_d(p, s2);
+          __syncthreads();
+          tile_mm<T, NB>(Bs, LT, Xb(s2, q), LX, Tt, LT, T(1), s2 > q);
+        }
+        __syncthreads();
+        tile_mm<T, NB>(As, LT, Tt, LT, Xb(p, q), LX, T(-1), false);
+      }
+    } else {
+      for (int q = p - 1; q >= 0; --q) {
+        // Tt = sum_{s=q+1}^{p} U[q][s] Y[s][p];  Y[q][p] = -Uinv_q Tt
+        for (int s2 = q + 1; s2 <= p; ++s2) {
+          __syncthreads();
+          stage_d(q, s2);
+          __syncthreads();
+          tile_mm<T, NB>(Bs, LT, Xb(s2, p), LX, Tt, LT, T(1), s2 > q + 1);
+        }
+        __syncthreads();
+        stage_inv(pbase + q);
+        __syncthreads();
+        tile_mm<T, NB>(As, LT, Tt, LT, Xb(q, p), LX, T(-1), false);
+      }
+    }
+  }
+  __syncthreads();
+  // zero outside the leaf's part of the block (rows / columns >= obe)
+  T *dst = (upper ? tk.UinvB : tk.LinvB) + (size_t)J * ob * ob;
+  for (int e = tid; e < ob * ob; e += kInvThreads) {
+    const int i = e % ob, c = e / ob;
+    dst[e] = (i < obe && c < obe) ? X[i + c * LX] : T(0);
+  }
+}
+
 }  // namespace
 
 template <int NB, typename T>
@@ -846,6 +969,30 @@ void launch_leaf_apply(const LeafFactorTask<T> *tasks, int count, int max_n, int
   else if (max_cols <= 16 || !wide_ok) launch_leaf_apply_mc<T, 16>(tasks, count, max_n, max_cols, nb, s);
   else launch_leaf_apply_mc<T, 32>(tasks, count, max_n, max_cols, nb, s);
 }
+
+template <typename T>
+void launch_leaf_block_inverse(const LeafFactorTask<T> *tasks, int count, int nb, int ob, int J,
+                               cudaStream_t s) {
+  if (count <= 0) return;
+  if (ob > 128 || ob % nb) throw CudaError{cudaErrorInvalidValue};
+  dim3 grid(count, 2);
+  auto go = [&](auto kern, int NBv) {
+    const size_t smem = ((size_t)ob * (ob + 1) + 3 * (size_t)NBv * (NBv + 1)) * sizeof(T);
+    HODLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    kern<<<grid, kInvThreads, smem, s>>>(tasks, ob, J);
+  };
+  if (nb == 64) go(leaf_block_inverse_kernel<T, 64>, 64);
+  else if (nb == 32) go(leaf_block_inverse_kernel<T, 32>, 32);
+  else if (nb == 16) go(leaf_block_inverse_kernel<T, 16>, 16);
+  else throw CudaError{cudaErrorInvalidValue};
+  HODLR_LAUNCH_CHECK();
+}
+
+template void launch_leaf_block_inverse<double>(const LeafFactorTask<double> *, int, int, int,
+                                                int, cudaStream_t);
+template void launch_leaf_block_inverse<float>(const LeafFactorTask<float> *, int, int, int, int,
+                                               cudaStream_t);
 
 template void launch_leaf_apply<double>(const LeafFactorTask<double> *, int, int, int, int,
                                         cudaStream_t);

@@ -22,6 +22,8 @@ struct LeafFactorTask {
   T *Linv;         // npanels x NB x NB: inverses of the unit-lower diagonal blocks
   T *Uinv;         // npanels x NB x NB: inverses of the upper diagonal blocks
   int *swapflag;   // npanels: panel had row interchanges
+  T *LinvB;        // nblocks x OB x OB: inverses of the unit-lower outer diagonal blocks
+  T *UinvB;        // nblocks x OB x OB: inverses of the upper outer diagonal blocks
   long long ldd;
   long long ldx;
   int n;
@@ -39,6 +41,13 @@ void launch_leaf_apply(const LeafFactorTask<T> *tasks, int count, int max_n, int
 
 template <typename T>
 void launch_leaf_init(const LeafFactorTask<T> *tasks, int count, int *info, cudaStream_t s);
+// Inverses of outer block J's unit-lower and upper diagonal blocks (ob x ob,
+// ob a multiple of nb and at most 128) from the block's factored panels and
+// their nb x nb inverses, into task.LinvB / task.UinvB + J ob^2 (column-major,
+// ld ob, zero outside the leaf).
+template <typename T>
+void launch_leaf_block_inverse(const LeafFactorTask<T> *tasks, int count, int nb, int ob, int J,
+                               cudaStream_t s);
 template <typename T>
 void launch_leaf_panel(const LeafFactorTask<T> *tasks, int count, int max_n, int nb, int k0,
                        int panel, int *info, cudaStream_t s);

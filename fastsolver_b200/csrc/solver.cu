@@ -105,6 +105,13 @@ void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long
   lp.nblocks = cdiv(lp.max_n, OB);
   lp.Linv.ensure((size_t)nleaf * max_panels * NB * NB);
   lp.Uinv.ensure((size_t)nleaf * max_panels * NB * NB);
+  // block-row solves by the inverses of the outer diagonal blocks: in place
+  // on the block's rows, which one GEMM tile row (128) covers
+  const bool binv = P > 1 && OB <= 128;
+  if (binv) {
+    lp.LinvB.ensure((size_t)nleaf * lp.nblocks * OB * OB);
+    lp.UinvB.ensure((size_t)nleaf * lp.nblocks * OB * OB);
+  }
   lp.swapflag.ensure((size_t)nleaf * max_panels);
   std::vector<LeafFactorTask<T>> tasks(nleaf);
   lp.laswp_cols = 0;
@@ -120,6 +127,8 @@ void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long
     k.Linv = lp.Linv.p + (size_t)q * max_panels * NB * NB;
     k.Uinv = lp.Uinv.p + (size_t)q * max_panels * NB * NB;
     k.swapflag = lp.swapflag.p + (size_t)q * max_panels;
+    k.LinvB = binv ? lp.LinvB.p + (size_t)q * lp.nblocks * OB * OB : nullptr;
+    k.UinvB = binv ? lp.UinvB.p + (size_t)q * lp.nblocks * OB * OB : nullptr;
     k.n = nd.nrow;
     k.ncols = factor_cols_all ? nd.col_beg + nd.ncol : m;
     k.info_slot = q;
@@ -187,8 +196,27 @@ void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long
     }
     // the block's interchanges on the columns left and right of it and on X
     lp.fwd.push_back(laswp_step(J * P, P, 0, j0, j0 + OB, kAll, true));
+    if (binv) {
+      // block rows: U12 = L11^{-1} A12 on R = (D right of the block | X), one
+      // product with the inverse of the block's unit-lower triangle
+      auto inv = std::make_unique<Step>();
+      inv->kind = LeafPlan<T>::kBlockInv;
+      inv->block = J;
+      lp.fwd.push_back(std::move(inv));
+      Acc tr;
+      for (const LeafFactorTask<T> &k : tasks) {
+        if (j0 >= k.n) continue;
+        const int obe = std::min(OB, k.n - j0);
+        const T *Li = k.LinvB + (size_t)J * OB * OB;
+        T *Dr = k.D + j0 + (long long)(j0 + obe) * ldd;
+        T *Xr = k.X + j0;
+        tr.add(Dr, ldd, obe, k.n - j0 - obe, Li, OB, Dr, ldd, obe, false);
+        tr.add(Xr, ldx, obe, k.ncols, Li, OB, Xr, ldx, obe, false);
+      }
+      lp.fwd.push_back(gemm_step(LeafPlan<T>::kTrsm, tr));
+    }
     // block rows: U12 = L11^{-1} A12 by panels on R = (D right of the block | X)
-    for (int p = 0; p < P; ++p) {
+    for (int p = 0; p < (binv ? 0 : P); ++p) {
       const int pi = J * P + p, k0 = pi * NB;
       Acc tr, up;
       for (const LeafFactorTask<T> &k : tasks) {
@@ -222,11 +250,22 @@ void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long
     }
     lp.fwd.push_back(gemm_step(LeafPlan<T>::kUpdate, big));
   }
-  lp.fwd_per_block = 6 * P + 2;
+  lp.fwd_per_block = binv ? 4 * P + 4 : 6 * P + 2;
   // backward solve on X, last block first
   for (int J = lp.nblocks - 1; J >= 0; --J) {
     const int j0 = J * OB;
-    for (int p = P - 1; p >= 0; --p) {
+    if (binv) {
+      // X[block] = U11^{-1} X[block]: one product with the block's upper inverse
+      Acc tr;
+      for (const LeafFactorTask<T> &k : tasks) {
+        if (j0 >= k.n) continue;
+        const int obe = std::min(OB, k.n - j0);
+        T *Xk = k.X + j0;
+        tr.add(Xk, ldx, obe, k.ncols, k.UinvB + (size_t)J * OB * OB, OB, Xk, ldx, obe, false);
+      }
+      lp.bwd.push_back(gemm_step(LeafPlan<T>::kTrsm, tr));
+    }
+    for (int p = binv ? -1 : P - 1; p >= 0; --p) {
       const int pi = J * P + p, k0 = pi * NB;
       Acc tr, up;
       for (const LeafFactorTask<T> &k : tasks) {
@@ -248,7 +287,7 @@ void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long
     }
     lp.bwd.push_back(gemm_step(LeafPlan<T>::kUpdate, big));
   }
-  lp.bwd_per_block = 2 * P + 1;
+  lp.bwd_per_block = binv ? 2 : 2 * P + 1;
 }
 
 template <typename TA, typename TC, typename TACC>
@@ -514,6 +553,11 @@ void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t 
                              st.a1, st.b0, st.b1, st.with_x, s);
         break;
       }
+      case LeafPlan<T>::kBlockInv: {
+        PhaseScope pt(pf, PH_LEAF_TRSM, s);
+        launch_leaf_block_inverse<T>(lp.tasks.p, lp.nleaf, lp.nb, lp.ob, st.block, s);
+        break;
+      }
       case LeafPlan<T>::kTrsm: {
         if (st.g.n == 0) break;
         PhaseScope pt(pf, PH_LEAF_TRSM, s);
@@ -770,6 +814,7 @@ void merge_leaf_plans(const std::vector<const LeafPlan<T> *> &src, const std::ve
     st->kind = proto.kind;
     st->k0 = proto.k0;
     st->panel = proto.panel;
+    st->block = proto.block;
     st->np = proto.np;
     st->a0 = proto.a0; st->a1 = proto.a1; st->b0 = proto.b0; st->b1 = proto.b1;
     st->with_x = proto.with_x;

@@ -101,18 +101,23 @@ struct GemmLaunch {
 // panels whose row interchanges and updates stay inside the block's columns;
 // then the block's interchanges on the other columns, the block-row solve
 // and one trailing update of depth ob.  The backward solve on X runs by the
-// same blocks.  ob == nb is the one-level right-looking factorization.
+// same blocks.  With ob <= 128 the block-row solves (forward on the rows of
+// the block, backward on X) are single products with the inverses of the
+// block's triangles, built from the panels' inverses; larger blocks solve
+// panel by panel.  ob == nb is the one-level right-looking factorization.
 template <typename T>
 struct LeafPlan {
   DevBuf<LeafFactorTask<T>> tasks;
   DevBuf<T> Linv, Uinv;
+  DevBuf<T> LinvB, UinvB;  // outer-block inverses (two-level plans with ob <= 128)
   DevBuf<int> swapflag;
   std::vector<LeafFactorTask<T>> host_tasks;  // for apply plans with these factors
   int nleaf = 0, max_n = 0, laswp_cols = 0, nb = 0, ob = 0;
-  enum Kind { kPanel, kLaswp, kTrsm, kUpdate };
+  enum Kind { kPanel, kLaswp, kTrsm, kUpdate, kBlockInv };
   struct Step {
     Kind kind = kPanel;
     int k0 = 0, panel = 0;          // kPanel: the panel; kLaswp: first panel
+    int block = 0;                  // kBlockInv: the outer block
     int np = 0;                     // kLaswp: panels applied
     int a0 = 0, a1 = 0, b0 = 0, b1 = 0;  // kLaswp: D column ranges (clamped per leaf)
     bool with_x = false;            // kLaswp: X columns too
