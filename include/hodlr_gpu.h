@@ -287,7 +287,9 @@ int hodlr_batch_phase_times(hodlr_batch batch, double *ms, long long *launches, 
  *   leaf_nb      FP32 leaf panel width: 0 = by the largest leaf (64 up to 512
  *                rows, else 32), or 32, or 64 (leaves of <= 512 rows only);
  *   leaf_ob32    FP32 leaf outer block width (a multiple of the panel width,
- *                rounded down; 0 = one-level blocking);
+ *                rounded down; 0 = one-level blocking; blocks of at most 128
+ *                columns solve their block rows with the inverses of the
+ *                block's triangles, wider ones panel by panel);
  *   leaf_ob64    the same for the FP64 path (panel width 32, or 16 above 512
  *                rows);
  *   reduce_rows  rows per split-K slot of the reduce V^T [d | u] (16..65536,
