@@ -757,9 +757,11 @@ __global__ void __launch_bounds__(kApplyThreads)
 //   X[p][p] = Linv_p,  X[p][q] = -Linv_p sum_{s=q}^{p-1} L[p][s] X[s][q]  (q < p),
 // and the upper one by block back substitution from Uinv_p:
 //   Y[p][p] = Uinv_p,  Y[q][p] = -Uinv_q sum_{s=q+1}^{p} U[q][s] Y[s][p]  (q < p).
-// CTA (256 threads) = one leaf x {lower, upper}; the ob x ob result, an NB x NB
-// product tile and two staged NB x NB operands live in shared memory (padded
-// leading dimensions), products are 16 x 16 thread grids of R x R outputs.
+// Lower: CTA (256 threads) = one leaf, for one block; upper: one leaf x one
+// block, all blocks in one launch.  The ob x ob result, an NB x NB product
+// tile and one staged NB x NB block of D live in shared memory (padded leading
+// dimensions; the panel inverses are read from global memory), so two CTAs
+// fit on an SM; products are 16 x 16 thread grids of R x R outputs.
 constexpr int kInvThreads = 256;
 
 template <typename T, int NB>
@@ -795,29 +797,27 @@ __device__ inline void tile_mm(const T *A, int lda, const T *B, int ldb, T *C, i
 
 template <typename T, int NB>
 __global__ void __launch_bounds__(kInvThreads)
-    leaf_block_inverse_kernel(const LeafFactorTask<T> *__restrict__ tasks, int ob, int J) {
+    leaf_block_inverse_kernel(const LeafFactorTask<T> *__restrict__ tasks, int ob, int J0,
+                              int upper) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const LeafFactorTask<T> tk = tasks[blockIdx.x];
   const int n = tk.n;
+  const int J = upper ? (int)blockIdx.y : J0;  // upper: every block, one per grid row
   const int j0 = J * ob;
   if (j0 >= n) return;
   const int obe = min(ob, n - j0);
   const int P = (obe + NB - 1) / NB;
   const int pbase = j0 / NB;
-  const bool upper = blockIdx.y == 1;
   constexpr int LT = NB + 1;  // padded ld of the NB x NB tiles
   const int LX = ob + 1;      // padded ld of the block inverse
   T *X = reinterpret_cast<T *>(smem_raw);  // ob x ob
   T *Tt = X + (size_t)ob * LX;             // product tile
-  T *As = Tt + NB * LT;                    // staged panel inverse
-  T *Bs = As + NB * LT;                    // staged L / U block of D
+  T *Bs = Tt + NB * LT;                    // staged L / U block of D
   const int tid = threadIdx.x;
   for (int e = tid; e < ob * ob; e += kInvThreads) X[(e % ob) + (e / ob) * LX] = T(0);
-  // stage panel pi's inverse (NB x NB, ld NB; identity beyond the leaf)
-  auto stage_inv = [&](int pi) {
-    const T *src = (upper ? tk.Uinv : tk.Linv) + (size_t)pi * NB * NB;
-    for (int e = tid; e < NB * NB; e += kInvThreads) As[(e % NB) + (e / NB) * LT] = src[e];
-  };
+  // panel pi's inverse (NB x NB, ld NB; identity beyond the leaf), read from
+  // global memory (L1 / L2) by the products
+  auto inv_of = [&](int pi) { return (upper ? tk.Uinv : tk.Linv) + (size_t)pi * NB * NB; };
   // stage the NB x NB block of D at block panels (pr, pc), zero outside the block
   auto stage_d = [&](int pr, int pc) {
     for (int e = tid; e < NB * NB; e += kInvThreads) {
@@ -829,11 +829,12 @@ __global__ void __launch_bounds__(kInvThreads)
   auto Xb = [&](int pr, int pc) { return X + pr * NB + (size_t)pc * NB * LX; };
   for (int p = 0; p < P; ++p) {
     __syncthreads();
-    stage_inv(pbase + p);
-    __syncthreads();
-    for (int e = tid; e < NB * NB; e += kInvThreads) {
-      const int i = e % NB, c = e / NB;
-      if (p * NB + i < ob && p * NB + c < ob) Xb(p, p)[i + c * LX] = As[i + c * LT];
+    {
+      const T *src = inv_of(pbase + p);
+      for (int e = tid; e < NB * NB; e += kInvThreads) {
+        const int i = e % NB, c = e / NB;
+        Xb(p, p)[i + c * LX] = src[e];
+      }
     }
     if (!upper) {
       for (int q = 0; q < p; ++q) {
@@ -845,7 +846,7 @@ __global__ void __launch_bounds__(kInvThreads)
           tile_mm<T, NB>(Bs, LT, Xb(s2, q), LX, Tt, LT, T(1), s2 > q);
         }
         __syncthreads();
-        tile_mm<T, NB>(As, LT, Tt, LT, Xb(p, q), LX, T(-1), false);
+        tile_mm<T, NB>(inv_of(pbase + p), NB, Tt, LT, Xb(p, q), LX, T(-1), false);
       }
     } else {
       for (int q = p - 1; q >= 0; --q) {
@@ -857,9 +858,7 @@ __global__ void __launch_bounds__(kInvThreads)
           tile_mm<T, NB>(Bs, LT, Xb(s2, p), LX, Tt, LT, T(1), s2 > q + 1);
         }
         __syncthreads();
-        stage_inv(pbase + q);
-        __syncthreads();
-        tile_mm<T, NB>(As, LT, Tt, LT, Xb(q, p), LX, T(-1), false);
+        tile_mm<T, NB>(inv_of(pbase + q), NB, Tt, LT, Xb(q, p), LX, T(-1), false);
       }
     }
   }
@@ -972,15 +971,15 @@ void launch_leaf_apply(const LeafFactorTask<T> *tasks, int count, int max_n, int
 
 template <typename T>
 void launch_leaf_block_inverse(const LeafFactorTask<T> *tasks, int count, int nb, int ob, int J,
-                               cudaStream_t s) {
-  if (count <= 0) return;
+                               bool upper, int nblocks, cudaStream_t s) {
+  if (count <= 0 || (upper && nblocks <= 0)) return;
   if (ob > 128 || ob % nb) throw CudaError{cudaErrorInvalidValue};
-  dim3 grid(count, 2);
+  dim3 grid(count, upper ? nblocks : 1);
   auto go = [&](auto kern, int NBv) {
-    const size_t smem = ((size_t)ob * (ob + 1) + 3 * (size_t)NBv * (NBv + 1)) * sizeof(T);
+    const size_t smem = ((size_t)ob * (ob + 1) + 2 * (size_t)NBv * (NBv + 1)) * sizeof(T);
     HODLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
-    kern<<<grid, kInvThreads, smem, s>>>(tasks, ob, J);
+    kern<<<grid, kInvThreads, smem, s>>>(tasks, ob, J, upper ? 1 : 0);
   };
   if (nb == 64) go(leaf_block_inverse_kernel<T, 64>, 64);
   else if (nb == 32) go(leaf_block_inverse_kernel<T, 32>, 32);
@@ -990,9 +989,9 @@ void launch_leaf_block_inverse(const LeafFactorTask<T> *tasks, int count, int nb
 }
 
 template void launch_leaf_block_inverse<double>(const LeafFactorTask<double> *, int, int, int,
-                                                int, cudaStream_t);
+                                                int, bool, int, cudaStream_t);
 template void launch_leaf_block_inverse<float>(const LeafFactorTask<float> *, int, int, int, int,
-                                               cudaStream_t);
+                                               bool, int, cudaStream_t);
 
 template void launch_leaf_apply<double>(const LeafFactorTask<double> *, int, int, int, int,
                                         cudaStream_t);

@@ -41,13 +41,14 @@ void launch_leaf_apply(const LeafFactorTask<T> *tasks, int count, int max_n, int
 
 template <typename T>
 void launch_leaf_init(const LeafFactorTask<T> *tasks, int count, int *info, cudaStream_t s);
-// Inverses of outer block J's unit-lower and upper diagonal blocks (ob x ob,
-// ob a multiple of nb and at most 128) from the block's factored panels and
-// their nb x nb inverses, into task.LinvB / task.UinvB + J ob^2 (column-major,
-// ld ob, zero outside the leaf).
+// Inverse of outer block J's unit-lower diagonal block (ob x ob, ob a
+// multiple of nb and at most 128) from the block's factored panels and their
+// nb x nb inverses, into task.LinvB + J ob^2 (column-major, ld ob, zero
+// outside the leaf); with `upper`, the inverses of the upper diagonal blocks
+// of all `nblocks` blocks into task.UinvB (J unused).
 template <typename T>
 void launch_leaf_block_inverse(const LeafFactorTask<T> *tasks, int count, int nb, int ob, int J,
-                               cudaStream_t s);
+                               bool upper, int nblocks, cudaStream_t s);
 template <typename T>
 void launch_leaf_panel(const LeafFactorTask<T> *tasks, int count, int max_n, int nb, int k0,
                        int panel, int *info, cudaStream_t s);

@@ -108,6 +108,7 @@ void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long
   // block-row solves by the inverses of the outer diagonal blocks: in place
   // on the block's rows, which one GEMM tile row (128) covers
   const bool binv = P > 1 && OB <= 128;
+  lp.binv = binv;
   if (binv) {
     lp.LinvB.ensure((size_t)nleaf * lp.nblocks * OB * OB);
     lp.UinvB.ensure((size_t)nleaf * lp.nblocks * OB * OB);
@@ -555,7 +556,7 @@ void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t 
       }
       case LeafPlan<T>::kBlockInv: {
         PhaseScope pt(pf, PH_LEAF_TRSM, s);
-        launch_leaf_block_inverse<T>(lp.tasks.p, lp.nleaf, lp.nb, lp.ob, st.block, s);
+        launch_leaf_block_inverse<T>(lp.tasks.p, lp.nleaf, lp.nb, lp.ob, st.block, false, 0, s);
         break;
       }
       case LeafPlan<T>::kTrsm: {
@@ -576,6 +577,10 @@ void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t 
     PhaseScope ps(pf, PH_GETRF, s);
     launch_leaf_init<T>(lp.tasks.p, lp.nleaf, info, s);
     for (const auto &st : lp.fwd) run_step(*st);
+    if (lp.binv) {  // the upper block inverses of every block, for the backward solve
+      PhaseScope pt(pf, PH_LEAF_TRSM, s);
+      launch_leaf_block_inverse<T>(lp.tasks.p, lp.nleaf, lp.nb, lp.ob, 0, true, lp.nblocks, s);
+    }
   }
   {
     PhaseScope ps(pf, PH_GETRS, s);
@@ -801,6 +806,7 @@ void merge_leaf_plans(const std::vector<const LeafPlan<T> *> &src, const std::ve
   }
   dst.fwd_per_block = src[0]->fwd_per_block;
   dst.bwd_per_block = src[0]->bwd_per_block;
+  dst.binv = src[0]->binv;
   dst.tasks.upload(tasks);
   dst.host_tasks = tasks;
   dst.nleaf = (int)tasks.size();

@@ -127,6 +127,7 @@ struct LeafPlan {
   // bwd: the steps of the last block first (bwd_per_block each)
   std::vector<std::unique_ptr<Step>> fwd, bwd;
   int nblocks = 0, fwd_per_block = 0, bwd_per_block = 0;
+  bool binv = false;  // block rows solved with the outer blocks' inverses
 };
 
 template <typename T, typename TE>
