@@ -990,6 +990,7 @@ int System::init(int N_, int nrhs, int rank, int threshold) {
   R64.ensure(n * m);
   MVx.ensure(n * m);
   relres_dev.ensure(m);
+  ratio_part.ensure((size_t)m * kRatioChunks * 2);
   n_info = (int)(tree.leaves.size() + tree.nodes.size());
   info.ensure(n_info);
   HODLR_CUDA_TRY(cudaMemset(info.p, 0, sizeof(int) * n_info));
@@ -1117,7 +1118,7 @@ int System::check_info(cudaStream_t s) {
 
 void System::relres_enqueue(cudaStream_t s) {
   run_matvec(mv_sol, -1.0, 1.0, s);
-  launch_colratio(R64.p, N, B.p, N, N, m, relres_dev.p, s);
+  launch_colratio(R64.p, N, B.p, N, N, m, ratio_part.p, relres_dev.p, s);
 }
 
 double System::relres(cudaStream_t s) {

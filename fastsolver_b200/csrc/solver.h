@@ -236,7 +236,7 @@ struct System {
   // mixed path
   DevBuf<float> X32, D32, V32, Y32;
   DevBuf<int> ipiv32, perm32;
-  DevBuf<double> R64, MVx, relres_dev;
+  DevBuf<double> R64, MVx, relres_dev, ratio_part;
   // workspaces
   DevBuf<double> part64, wfin64, eta64, tbuf, mvpart;
   DevBuf<float> part32, wfin32, eta32;

@@ -96,14 +96,16 @@ void launch_ew_tile(const TS *src, long long lds, TD *dst, long long ldd, long l
   HODLR_LAUNCH_CHECK();
 }
 
-// out[c] = sqrt(sum_i r(i,c)^2) / sqrt(sum_i b(i,c)^2), one CTA per column.
-__global__ void colratio_kernel(const double *__restrict__ r, long long ldr,
-                                const double *__restrict__ b, long long ldb, long long rows,
-                                double *__restrict__ out) {
+// Sums of squares of r(:, c) and b(:, c) over one row chunk: CTA (c, chunk).
+__global__ void colratio_part_kernel(const double *__restrict__ r, long long ldr,
+                                     const double *__restrict__ b, long long ldb, long long rows,
+                                     double *__restrict__ part) {
   __shared__ double sr[32], sb[32];
-  const int c = blockIdx.x;
+  const int c = blockIdx.x, q = blockIdx.y, nq = gridDim.y;
+  const long long len = (rows + nq - 1) / nq;
+  const long long i0 = q * len, i1 = min(rows, i0 + len);
   double ar = 0.0, ab = 0.0;
-  for (long long i = threadIdx.x; i < rows; i += blockDim.x) {
+  for (long long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
     const double x = r[i + c * ldr], y = b[i + c * ldb];
     ar += x * x;
     ab += y * y;
@@ -117,9 +119,24 @@ __global__ void colratio_kernel(const double *__restrict__ r, long long ldr,
   if (threadIdx.x == 0) {
     double tr = 0.0, tb = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { tr += sr[w]; tb += sb[w]; }
-    out[c] = tb > 0.0 ? sqrt(tr) / sqrt(tb) : sqrt(tr);
+    part[2 * ((long long)c * nq + q)] = tr;
+    part[2 * ((long long)c * nq + q) + 1] = tb;
   }
 }
+
+// out[c] from the chunk sums, added in chunk order: one thread per column.
+__global__ void colratio_fin_kernel(const double *__restrict__ part, int nq, int cols,
+                                    double *__restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  double tr = 0.0, tb = 0.0;
+  for (int q = 0; q < nq; ++q) {
+    tr += part[2 * ((long long)c * nq + q)];
+    tb += part[2 * ((long long)c * nq + q) + 1];
+  }
+  out[c] = tb > 0.0 ? sqrt(tr) / sqrt(tb) : sqrt(tr);
+}
+
 
 // Batched element-wise pass: one grid-stride loop over the tiles of all
 // tasks (a tile = 1024 rows of one column; tile -> task by binary search on
@@ -149,7 +166,8 @@ __global__ void ew2d_batched_kernel(const Ew2DTask<TS, TD> *__restrict__ tasks, 
   }
 }
 
-// Batched colratio_kernel: blockIdx.y picks the system, blockIdx.x the column.
+// Batched column ratios (one CTA per column; batches supply many columns):
+// blockIdx.y picks the system, blockIdx.x the column.
 __global__ void colratio_batched_kernel(const RatioTask *__restrict__ tasks) {
   __shared__ double sr[32], sb[32];
   const RatioTask tk = tasks[blockIdx.y];
@@ -377,9 +395,12 @@ template void launch_add2d<double>(double *, long long, const double *, long lon
                                    long long, cudaStream_t);
 
 void launch_colratio(const double *r, long long ldr, const double *b, long long ldb,
-                     long long rows, int cols, double *out, cudaStream_t s) {
+                     long long rows, int cols, double *part, double *out, cudaStream_t s) {
   if (cols <= 0) return;
-  colratio_kernel<<<cols, 1024, 0, s>>>(r, ldr, b, ldb, rows, out);
+  const int nq = (int)std::max<long long>(1, std::min<long long>(kRatioChunks, (rows + 4095) / 4096));
+  colratio_part_kernel<<<dim3(cols, nq), 256, 0, s>>>(r, ldr, b, ldb, rows, part);
+  HODLR_LAUNCH_CHECK();
+  colratio_fin_kernel<<<(cols + 127) / 128, 128, 0, s>>>(part, nq, cols, out);
   HODLR_LAUNCH_CHECK();
 }
 

@@ -24,8 +24,13 @@ void launch_convert2d(const TS *src, long long lds, TD *dst, long long ldd, long
 template <typename TS>
 void launch_add2d(double *x, long long ldx, const TS *y, long long ldy, long long rows,
                   long long cols, cudaStream_t s);
+// out[c] = ||r(:, c)|| / ||b(:, c)|| (||r(:, c)|| where b(:, c) = 0), c < cols:
+// every column is cut into up to kRatioChunks row chunks whose sums of
+// squares land in `part` (cols x kRatioChunks x 2 doubles of scratch) and are
+// added in a fixed order (deterministic).
+constexpr int kRatioChunks = 64;
 void launch_colratio(const double *r, long long ldr, const double *b, long long ldb,
-                     long long rows, int cols, double *out, cudaStream_t s);
+                     long long rows, int cols, double *part, double *out, cudaStream_t s);
 template <typename T>
 void launch_sum_slots(const SumTask<T> *tasks, int ntasks, long long max_len, cudaStream_t s);
 void launch_scale_cols(double *a, long long lda, long long rows, int cols, const double *s_dev,
