@@ -32,7 +32,7 @@ namespace hodlr {
 
 namespace {
 
-constexpr int kNodeThreads = 256;
+constexpr int kNodeThreads = 512;
 constexpr int kNodeWarps = kNodeThreads / 32;
 
 }  // namespace
