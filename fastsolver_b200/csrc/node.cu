@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(kNodeThreads)
   // Rows never move; every warp finds the pivot of column k itself (largest
   // |a| among the rows not yet pivotal, lowest current position on ties, as
   // idamax after LAPACK's interchanges) and keeps identical copies of the
-  // rows' current positions.  Warp w eliminates column k from rows w, w + 8,
+  // rows' current positions.  Warp w eliminates column k from rows w, w + kNodeWarps,
   // ... with the (unscaled) pivot row; the pivot row itself is scaled by its
   // owner at the start of the next step, when nobody else reads it.
   // RL: rows (and columns) per lane, ceil(max_s / 32)
