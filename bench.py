@@ -335,6 +335,7 @@ def run_batch(args):
     clk = clocks.stop()
     sweeps = [o[0] for o in outs]
     rr_max = max(max(o[1]) for o in outs)
+    x_batch = [h.solution(stream=stream) for h in hs]   # outside the timed region
 
     def seq_mixed():
         return [solver.solve_refined(h, fs.PREC_MIXED, tol=TOL, maxiter=10, stream=stream)
@@ -361,6 +362,31 @@ def run_batch(args):
     batch_step()
     ph = batch.phase_times(reset=True)
     batch.set_profiling(False)
+
+    # the oracle (restated reference FP64 walk) on the host cores: systems of
+    # the draw one after another, in draw order, until about args.cpu_seconds
+    # of CPU time; the batched solutions' forward error against its solutions
+    cpu, fwd = None, None
+    if not args.no_cpu_baseline and rank == 0:
+        from oracle import refcpu as R
+        threads = os.cpu_count() or 1
+        R.lib().ref_set_blas_threads(1)
+        errs, t_cpu, n_cpu = [], 0.0, 0
+        for i, h in enumerate(hs):
+            if t_cpu > args.cpu_seconds:
+                break
+            D, U, V, B = h.get_matrix()
+            so = R.System(h.tree_nodes(), D, U, V, B)
+            t0 = time.perf_counter()
+            Xc, _ = R.bfs_solve(so, nthreads=threads)
+            t_cpu += time.perf_counter() - t0
+            n_cpu += 1
+            errs.append(R.rel_error(x_batch[i], Xc[:, : cfgs[i]["nrhs"]]))
+        cpu = {"value": n_cpu / t_cpu, "unit": "systems/s", "cores": threads, "kind": "port",
+               "sample": f"the first {n_cpu} of the {len(hs)} systems, fused FP64 solves one "
+                         "after another (oracle/refcpu.c, OpenBLAS, one OpenMP task per "
+                         "leaf/node)"}
+        fwd = {"batched_mixed_vs_oracle_max": max(errs), "systems_checked": n_cpu}
     if rank == 0:
         n = len(hs)
         line = {
@@ -384,7 +410,8 @@ def run_batch(args):
             "phases_ms": {k: round(v[0], 4) for k, v in ph.items()},
             "schedule": hs[0].schedule, "autotune": tune_info,
             "gpu_launches": int(launches), "clocks": clk,
-            "e2e": None, "cpu_baseline": None,
+            "forward_err": fwd,
+            "e2e": None, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     batch.close()
@@ -445,6 +472,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-solves", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0,
+                    help="CPU time budget of the batched workload's oracle sample")
+    ap.add_argument("--cpu-baseline-large", action="store_true",
+                    help="run the oracle leg also above N = 2^18 (needs ~40 GB of host "
+                         "memory at N = 2^20)")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch schedule (skip the autotuner)")
     ap.add_argument("--schedule", default=None,
@@ -553,6 +585,7 @@ def main():
     clk = clocks.stop()
     ms_mixed = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     barrier()
+    x_mixed = h.solution(stream=stream)   # the last timed solve's x (outside the timing)
 
     # ---- timed: plain FP64 path
     h.schedule = sched["fp64"]
@@ -567,6 +600,7 @@ def main():
     torch.cuda.synchronize()
     ms_fp64 = max_over_ranks(e0.elapsed_time(e1) / args.steps)
     rr_fp64 = h.relres(stream=stream)
+    x_fp64 = h.solution(stream=stream)
 
     # ---- per-phase device time (separate, event-bracketed passes)
     h.set_profiling(True)
@@ -661,8 +695,21 @@ def main():
         return t * 1e3 / ms
 
     total_flops = sum(W.values())
+
+    def rel(x, ref):
+        return float(np.linalg.norm(x - ref) / np.linalg.norm(ref))
+
+    # forward error (the reference's Err formula, direct_solve.cc:216-225):
+    # the mixed solution against the FP64 GPU solution always, and both
+    # against the oracle's FP64 solve of the same system with the CPU leg
+    fwd = {"mixed_vs_fp64_gpu": rel(x_mixed, x_fp64)}
+    relres_oracle = None
     cpu = None
-    if not args.no_cpu_baseline and ws == 1:
+    # the oracle holds the system and its working arrays in host memory
+    # (~40 GB at N = 2^20), so by default its leg runs up to N = 2^18
+    cpu_leg = (not args.no_cpu_baseline and ws == 1
+               and (cfg["N"] <= 262144 or args.cpu_baseline_large))
+    if cpu_leg:
         from oracle import refcpu as R
         D, U, V, B = h.get_matrix()
         s = R.System(tree, D, U, V, B)
@@ -676,6 +723,11 @@ def main():
                "kind": "port",
                "sample": f"{args.cpu_solves} full fused FP64 solves of the same system "
                          "(oracle/refcpu.c, OpenBLAS, one OpenMP task per leaf/node)"}
+        Xo = Xc[:, : cfg["nrhs"]]
+        fwd["mixed_vs_oracle"] = R.rel_error(x_mixed, Xo)
+        fwd["fp64_vs_oracle"] = R.rel_error(x_fp64, Xo)
+        relres_oracle = {"mixed": R.relres(s, x_mixed), "fp64": R.relres(s, x_fp64),
+                         "oracle": R.relres(s, Xo)}
 
     value = replica_value(ms_mixed, ws)
     line = {
@@ -688,6 +740,7 @@ def main():
                    **cfg, "levels": int(tree[:, 7].max()), "l2": "inputs 3.5 GB > L2",
                    "parallelism": f"replicas x{ws}"},
         "relres_max": float(max(rrs)), "refine_sweeps": iters,
+        "forward_err": fwd, "relres_oracle": relres_oracle,
         "fp64_gpu": {"value": replica_value(ms_fp64, ws), "unit": "solves/s", "ms_per_step": ms_fp64,
                      "relres": rr_fp64,
                      "roofline_frac": solve_frac(ms_fp64, 8, fp64_peak),

@@ -19,6 +19,7 @@ ERR_STATE = -1002
 ERR_NOCONV = -1003
 ERR_TIMEOUT = -1004
 ERR_UNSUPPORTED = -1005
+ERR_IO = -1006
 PREC_FP64 = 0
 PREC_MIXED = 1
 
@@ -88,6 +89,16 @@ _SIGS = {
     "hodlr_launch_count": [],
     "hodlr_reset_launch_count": [],
     "hodlr_status_string": [_i],
+    "hodlr_debug_tc_wait_hook": [_ll, _i],
+    "hodlr_set_leaf_size": [_vp, _i],
+    "hodlr_get_num_leaf": [_vp],
+    "hodlr_legion_leaves": [_vp, _ip, _i],
+    "hodlr_text_write": [ctypes.c_char_p, _vp, _ll, _i, _i, _i, ctypes.c_long, _i],
+    "hodlr_text_read": [ctypes.c_char_p, _vp, _ll, _i, _i, _i, _ip,
+                        ctypes.POINTER(ctypes.c_long)],
+    "hodlr_save_rhs": [_vp, ctypes.c_char_p, ctypes.c_long],
+    "hodlr_save_solution": [_vp, ctypes.c_char_p],
+    "hodlr_load_rhs": [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_long)],
 }
 
 

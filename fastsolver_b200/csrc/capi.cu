@@ -3,7 +3,10 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "gemm_simt.cuh"
@@ -23,17 +26,23 @@ void count_launch() { ++g_launches; }
 void add_launches(long long n) { g_launches += n; }
 long long launch_total() { return g_launches; }
 
+void raise_smem_limit(const void *func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> set;  // (function, device) -> limit
+  int dev = 0;
+  HODLR_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  size_t &cur = set[std::make_pair(func, dev)];
+  if (bytes <= cur) return;
+  HODLR_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)bytes));
+  cur = bytes;
+}
+
 }  // namespace hodlr
 
 using namespace hodlr;
 
-struct hodlr_system_s {
-  System sys;
-};
-
-struct hodlr_batch_s {
-  Batch b;
-};
 
 namespace {
 
@@ -70,6 +79,11 @@ struct StreamScratch {
   }
 };
 
+// HODLR_ERR_TIMEOUT if a tensor-core kernel's bounded wait gave up since the
+// flag was last read (the flag is sticky per device until read), else 0.
+// Call after the work has been synchronized.
+int tc_status() { return tc_error_flag(true) > 0 ? HODLR_ERR_TIMEOUT : 0; }
+
 int finish_info(int *info_user, int *info_dev, cudaStream_t s) {
   if (info_user) return 0;
   int h = 0;
@@ -94,6 +108,7 @@ const char *hodlr_status_string(int status) {
     case HODLR_ERR_NOCONV: return "refinement did not reach the tolerance";
     case HODLR_ERR_TIMEOUT: return "bounded device wait gave up";
     case HODLR_ERR_UNSUPPORTED: return "unsupported size or option";
+    case HODLR_ERR_IO: return "file could not be opened, read or written";
     default: break;
   }
   if (status > 0) return "zero pivot (LAPACK-style INFO)";
@@ -253,7 +268,16 @@ int hodlr_gemm_f32(int transa, int m, int n, int k, float alpha, const float *A,
     else
       launch_gemm_items<float, float, float>(di, ds, 1, m, n, transa != 0, alpha, beta, s, false);
     HODLR_CUDA_TRY(cudaStreamSynchronize(s));
-    return tc_error_flag(true) > 0 ? HODLR_ERR_TIMEOUT : 0;
+    return tc_status();
+  });
+}
+
+int hodlr_debug_tc_wait_hook(long long polls, int skip_one_commit) {
+  if (int e = device_ok()) return e;
+  return guarded([&]() -> int {
+    HODLR_CUDA_TRY(cudaDeviceSynchronize());
+    tc_set_wait_hook(polls, skip_one_commit);
+    return 0;
   });
 }
 
@@ -518,6 +542,14 @@ int hodlr_get_matrix(hodlr_system h, double *D, long long ldd, double *U, long l
   });
 }
 
+// (row_beg, rows) of every Legion leaf, left to right
+static std::vector<int2> legion_leaf_ranges(const System &S) {
+  std::vector<int2> v;
+  for (int id : legion_leaves(S.tree, S.leaf_size))
+    v.push_back(make_int2(S.tree.nodes[id].row_beg, S.tree.nodes[id].nrow));
+  return v;
+}
+
 static std::vector<int2> leaf_ranges(const Tree &t) {
   std::vector<int2> v;
   for (int id : t.leaves) v.push_back(make_int2(t.nodes[id].row_beg, t.nodes[id].nrow));
@@ -546,8 +578,9 @@ int hodlr_init_rhs_drand48(hodlr_system h, long seed, hodlr_stream_t stream) {
     System &S = h->sys;
     cudaStream_t s = as_stream(stream);
     DevBuf<int2> lv;
-    lv.upload(leaf_ranges(S.tree));
-    launch_drand48(lv.p, (int)S.tree.leaves.size(), S.B.p, S.N, S.m, seed, s);
+    const std::vector<int2> ranges = legion_leaf_ranges(S);
+    lv.upload(ranges);
+    launch_drand48(lv.p, (int)ranges.size(), S.B.p, S.N, S.m, seed, s);
     HODLR_CUDA_TRY(cudaStreamSynchronize(s));
     return 0;
   });
@@ -715,6 +748,36 @@ int hodlr_init_gaussian(hodlr_system h, unsigned long long seed, double offdiag_
   });
 }
 
+int hodlr_set_leaf_size(hodlr_system h, int leaf_size) {
+  if (!h) return -1;
+  if (leaf_size < 1) return -2;
+  System &S = h->sys;
+  if (leaf_size > 1 && 2 * S.r > kMaxNodeS) return HODLR_ERR_UNSUPPORTED;
+  if (leaf_size == S.leaf_size) return 0;
+  return guarded([&]() -> int {
+    S.leaf_size = leaf_size;
+    S.fused64[0].built = S.fused64[1].built = false;
+    S.reset_graphs();
+    if (S.factored == HODLR_PREC_FP64) S.factored = -1;
+    return 0;
+  });
+}
+
+int hodlr_get_num_leaf(hodlr_system h) {
+  if (!h) return -1;
+  return (int)legion_leaves(h->sys.tree, h->sys.leaf_size).size();
+}
+
+int hodlr_legion_leaves(hodlr_system h, int *ids, int cap) {
+  if (!h) return -1;
+  const std::vector<int> v = legion_leaves(h->sys.tree, h->sys.leaf_size);
+  if (ids) {
+    if (cap < (int)v.size()) return -3;
+    std::memcpy(ids, v.data(), sizeof(int) * v.size());
+  }
+  return (int)v.size();
+}
+
 int hodlr_solve_fused(hodlr_system h, int schur2, int sync, hodlr_stream_t stream) {
   if (!h) return -1;
   if (schur2 && 2 * h->sys.r > kMaxNodeS) return HODLR_ERR_UNSUPPORTED;
@@ -726,7 +789,11 @@ int hodlr_solve_fused(hodlr_system h, int schur2, int sync, hodlr_stream_t strea
     S.run_graph(S.g_fused64[form], s, [&]() { S.run_fused64(form, s); });
     S.factored = HODLR_PREC_FP64;
     S.factored_form = form;
-    if (sync) return S.check_info(s);
+    if (sync) {
+      const int info = S.check_info(s);
+      if (int t = tc_status()) return t;
+      return info;
+    }
     return 0;
   });
 }
@@ -738,7 +805,9 @@ int hodlr_factor(hodlr_system h, int precision, hodlr_stream_t stream) {
     cudaStream_t s = as_stream(stream);
     if (precision == HODLR_PREC_FP64) h->sys.run_fused64(0, s);
     else h->sys.run_factor32(s);
-    return h->sys.check_info(s);
+    const int info = h->sys.check_info(s);
+    if (int t = tc_status()) return t;
+    return info;
   });
 }
 
@@ -788,6 +857,8 @@ static int refined_body(System &S, int precision, double tol, int maxiter, int *
     S.factored_form = 0;
   }
   int info = S.check_info(s);
+  // a factor pass whose engine gave up is wrong: report that, not its INFO
+  if (int t = tc_status()) return t;
   if (info) return info;
   int it = 0;
   double rr = S.relres_read(s);
@@ -813,6 +884,7 @@ static int refined_body(System &S, int precision, double tol, int maxiter, int *
   }
   if (iters) *iters = it;
   if (relres) *relres = rr;
+  if (int t = tc_status()) return t;
   return rr <= tol ? 0 : HODLR_ERR_NOCONV;
 }
 
@@ -1087,6 +1159,7 @@ static int batch_body(Batch &B, double tol, int maxiter, int *iters, double *rel
     S->factored_form = 0;
   }
   int info = B.check_info(s, failed);
+  if (int t = tc_status()) return t;
   if (info) return info;
   std::vector<double> per;
   int it = 0;
@@ -1096,6 +1169,7 @@ static int batch_body(Batch &B, double tol, int maxiter, int *iters, double *rel
     ++it;
     rr = B.relres_read(s, &per);
   }
+  if (int t = tc_status()) return t;
   if (iters) *iters = it;
   if (relres_max) *relres_max = rr;
   if (relres)

@@ -43,6 +43,13 @@ inline cudaStream_t as_stream(hodlr_stream_t s) {
   return reinterpret_cast<cudaStream_t>(s);
 }
 
+// Raises `func`'s dynamic shared-memory limit on the current device to at
+// least `bytes` and never lowers it.  The limit is a property of the
+// function, not of a launch or of a captured graph node: lowering it for a
+// small launch would make an earlier-captured node that needs more fail at
+// replay, so every launch site goes through this one monotonic setter.
+void raise_smem_limit(const void *func, size_t bytes);
+
 // ---------------------------------------------------------------------------
 // Scalar helpers
 // ---------------------------------------------------------------------------

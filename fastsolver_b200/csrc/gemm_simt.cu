@@ -426,8 +426,7 @@ void launch_gemm_items(const GemmItem<TA, TC> *items, const GemmSeg<TA> *segs, i
     if (trans) {
       dim3 grid(nitems, cdiv(max_m, 64), cdiv(max_n, 16));
       const size_t red = 8 * 64 * 16 * sizeof(TACC);
-      HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_tn_kernel<TA, TC, TACC>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)red));
+      raise_smem_limit(reinterpret_cast<const void *>(skinny_tn_kernel<TA, TC, TACC>), red);
       skinny_tn_kernel<TA, TC, TACC><<<grid, NT, red, s>>>(items, segs, alpha, beta);
     } else {
       dim3 grid(nitems, cdiv(max_m, NT));

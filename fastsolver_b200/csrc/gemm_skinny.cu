@@ -605,8 +605,7 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
     // FP64 products run on the FP64 tensor pipe (DMMA)
     if (trans) {
       const size_t smem = (size_t)kSkStages * (64 + 16) * kDmmaLDK * sizeof(double);
-      HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_tn_dmma_kernel,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      raise_smem_limit(reinterpret_cast<const void *>(skinny_tn_dmma_kernel), smem);
       dim3 grid(nitems, cdiv(max_m, 64), cdiv(max_n, 16));
       skinny_tn_dmma_kernel<<<grid, kTNThreads, smem, s>>>(items, segs, alpha, beta);
     } else {
@@ -614,8 +613,7 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
       dim3 grid(nitems, cdiv(max_m, kDmmaRows), max_n <= 8 ? 1 : cdiv(max_n, 16));
       auto go = [&](auto kern, int ncs) {
         const size_t smem = (size_t)kDmmaStages * kDmmaKT * (kDmmaAP + ncs) * sizeof(double);
-        HODLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem));
+        raise_smem_limit(reinterpret_cast<const void *>(kern), smem);
         kern<<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);
       };
       if (max_n <= 8) go(skinny_nn_dmma_kernel<1>, 8);
@@ -627,8 +625,7 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
   if (trans) {
     constexpr int TM = 64, TN = 16, KC = 32, LDK = KC + 16 / sizeof(T);
     const size_t smem = (size_t)kSkStages * (TM + TN) * LDK * sizeof(T);
-    HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_tn2_kernel<T>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raise_smem_limit(reinterpret_cast<const void *>(skinny_tn2_kernel<T>), smem);
     dim3 grid(nitems, cdiv(max_m, TM), cdiv(max_n, TN));
     skinny_tn2_kernel<T><<<grid, kTNThreads, smem, s>>>(items, segs, alpha, beta);
   } else if constexpr (sizeof(T) == 4) {
@@ -643,13 +640,11 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
     dim3 grid(nitems, cdiv(max_m, kNNRows));
     if (max_n <= 16) {
       const size_t smem = (size_t)nn_stages<T>() * KT * (kNNRows + 16) * sizeof(T);
-      HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_nn2_kernel<T, 16>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      raise_smem_limit(reinterpret_cast<const void *>(skinny_nn2_kernel<T, 16>), smem);
       skinny_nn2_kernel<T, 16><<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);
     } else {
       const size_t smem = (size_t)nn_stages<T>() * KT * (kNNRows + 32) * sizeof(T);
-      HODLR_CUDA_TRY(cudaFuncSetAttribute(skinny_nn2_kernel<T, 32>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      raise_smem_limit(reinterpret_cast<const void *>(skinny_nn2_kernel<T, 32>), smem);
       skinny_nn2_kernel<T, 32><<<grid, kSkThreads, smem, s>>>(items, segs, alpha, beta);
     }
   }

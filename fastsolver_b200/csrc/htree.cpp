@@ -51,7 +51,25 @@ int build_tree(int N, int nrhs, int rank, int threshold, Tree &t) {
     t.ncols = std::max(t.ncols, n.col_beg + n.ncol);
     t.max_leaf = std::max(t.max_leaf, n.nrow);
   }
+  // real leaves per subtree: children come after their parent in BFS order
+  t.nreal.assign(t.nodes.size(), 0);
+  for (int i = (int)t.nodes.size() - 1; i >= 0; --i) {
+    const Node &n = t.nodes[i];
+    t.nreal[i] = n.is_leaf ? 1 : t.nreal[n.lchild] + t.nreal[n.rchild];
+  }
   return 0;
+}
+
+std::vector<int> legion_leaves(const Tree &t, int leaf_size) {
+  std::vector<int> out;
+  std::function<void(int)> walk = [&](int i) {
+    const Node &n = t.nodes[i];
+    if (t.nreal[i] <= leaf_size) { out.push_back(i); return; }
+    walk(n.lchild);
+    walk(n.rchild);
+  };
+  if (!t.nodes.empty()) walk(0);
+  return out;
 }
 
 }  // namespace hodlr

@@ -41,6 +41,7 @@ struct Tree {
   int max_leaf = 0;  // largest leaf row count
   std::vector<int> leaves;                          // leaf ids, left to right
   std::vector<std::vector<int>> internal_at_depth;  // internal node ids by depth
+  std::vector<int> nreal;                           // real leaves in each node's subtree
   int vcols() const { return ncols - nrhs; }
 };
 
@@ -48,5 +49,21 @@ struct Tree {
 // -4 threshold; -4 also when a leaf would not exceed the rank, which the
 // reference asserts at hodlr_matrix.cc:167).
 int build_tree(int N, int nrhs, int rank, int threshold, Tree &t);
+
+// Legion leaves at granularity `leaf_size` (>= 1), left to right: the
+// topmost nodes whose subtree holds at most leaf_size real leaves
+// (mark_legion_leaf, hodlr_matrix.cc:317-337).  With leaf_size == 1 they are
+// the real leaves.  A Legion leaf is one task of the reference: its
+// right-hand side is generated from one drand48 stream (init_matrix_tasks.cc:
+// 43-77), it is written as one block of the text output
+// (save_region_task.cc:37-67), and every internal node inside it is solved
+// with the 2r x 2r form of the leaf-internal branch (solver_tasks.cc:452-549)
+// instead of LUSolveTask's r x r form.
+std::vector<int> legion_leaves(const Tree &t, int leaf_size);
+
+// True if internal node `id` lies inside a Legion leaf (is one or is below one).
+inline bool inside_legion_leaf(const Tree &t, int id, int leaf_size) {
+  return t.nreal[id] <= leaf_size;
+}
 
 }  // namespace hodlr

@@ -358,8 +358,7 @@ void launch_getrf_pw(const LeafTask<T> *tasks, const LeafTask<T> &single, int co
                      int max_n, int *info, cudaStream_t s) {
   const int ps = (max_n + 3) & ~3;
   const size_t smem = getrf_smem<T, PW>(ps);
-  HODLR_CUDA_TRY(cudaFuncSetAttribute(getrf_kernel<T, PW>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit(reinterpret_cast<const void *>(getrf_kernel<T, PW>), smem);
   getrf_kernel<T, PW><<<count, kGetrfThreads, smem, s>>>(tasks, single, info, ps);
   HODLR_LAUNCH_CHECK();
 }
@@ -374,8 +373,7 @@ void launch_getrs_w(const LeafTask<T> *tasks, const LeafTask<T> &single, int cou
                     int max_n, int max_nrhs, cudaStream_t s) {
   const size_t smem =
       (size_t)max_n * (W + 2) * sizeof(T) + kBK * kBK * sizeof(T) + (size_t)max_n * sizeof(int);
-  HODLR_CUDA_TRY(cudaFuncSetAttribute(getrs_kernel<T, W>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit(reinterpret_cast<const void *>(getrs_kernel<T, W>), smem);
   dim3 grid(cdiv(max_nrhs, W), count);
   getrs_kernel<T, W><<<grid, kGetrsThreads, smem, s>>>(tasks, single);
   HODLR_LAUNCH_CHECK();

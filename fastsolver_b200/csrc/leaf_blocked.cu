@@ -893,8 +893,7 @@ void launch_leaf_panel_nb(const LeafFactorTask<T> *tasks, int count, int max_n, 
   // the panel buffer doubles as the inverses' output (2 NB^2 elements)
   const int psz = ps < 2 * NB ? 2 * NB : ps;
   const size_t smem = panel_smem<NB, T>(psz);
-  HODLR_CUDA_TRY(cudaFuncSetAttribute(leaf_panel_kernel<T, NB>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit(reinterpret_cast<const void *>(leaf_panel_kernel<T, NB>), smem);
   leaf_panel_kernel<T, NB><<<count, kThreads, smem, s>>>(tasks, k0, panel, psz, info);
   HODLR_LAUNCH_CHECK();
 }
@@ -949,8 +948,7 @@ void launch_leaf_apply_mc(const LeafFactorTask<T> *tasks, int count, int max_n, 
                           int nb, cudaStream_t s) {
   constexpr int XS = MC + 16 / sizeof(T);
   const size_t smem = ((size_t)max_n * XS + 2 * (size_t)nb * (nb + 1)) * sizeof(T);
-  HODLR_CUDA_TRY(cudaFuncSetAttribute(leaf_apply_kernel<T, MC>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit(reinterpret_cast<const void *>(leaf_apply_kernel<T, MC>), smem);
   dim3 grid(cdiv(max_cols, MC), count);
   leaf_apply_kernel<T, MC><<<grid, kApplyThreads, smem, s>>>(tasks, nb, max_n);
   HODLR_LAUNCH_CHECK();
@@ -977,8 +975,7 @@ void launch_leaf_block_inverse(const LeafFactorTask<T> *tasks, int count, int nb
   dim3 grid(count, upper ? nblocks : 1);
   auto go = [&](auto kern, int NBv) {
     const size_t smem = ((size_t)ob * (ob + 1) + 2 * (size_t)NBv * (NBv + 1)) * sizeof(T);
-    HODLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem));
+    raise_smem_limit(reinterpret_cast<const void *>(kern), smem);
     kern<<<grid, kInvThreads, smem, s>>>(tasks, ob, J, upper ? 1 : 0);
   };
   if (nb == 64) go(leaf_block_inverse_kernel<T, 64>, 64);

@@ -142,9 +142,10 @@ extern "C" int hodlr_gemm_reduce_noalloc(double alpha, int k, int r, int ncol, c
   if (col_beg < 0) return -9;
   if (!W && r > 0 && ncol > 0) return -10;
   if (ldw < (r > 1 ? r : 1)) return -11;
-  if (r == 0 || ncol == 0 || k == 0) return 0;
+  if (r == 0 || ncol == 0) return 0;
   const long long slot = (long long)r * ncol;
   if (slot > kNoAllocScratchDoubles) return HODLR_ERR_UNSUPPORTED;  // r * ncol > 2^20
+  if (k == 0) return 0;
   // as many row chunks as fit in the scratch, at least 1024 rows each
   long long nch = (k + 1023) / 1024;
   nch = std::min(nch, kNoAllocScratchDoubles / slot);

@@ -174,6 +174,9 @@ __global__ void __launch_bounds__(kNodeThreads)
   };
   for (int k = 0; k < s; ++k) {
     scale_prev();
+    // the owner warp's lanes wrote the previous pivot row, whose column k the
+    // same warp reads below (Ai[k] of its rows): order those accesses
+    __syncwarp();
     double best = 0.0;
     int bp = 0x7fffffff, code = -1;
 #pragma unroll
@@ -328,7 +331,7 @@ void launch_node_factor(const NodeTask<TW, TE> *tasks, int count, int max_s, int
   const int stage = (form == 0 && staged <= 200 * 1024) ? 1 : 0;
   if (stage) smem = staged;
   auto go = [&](auto kern) {
-    HODLR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raise_smem_limit(reinterpret_cast<const void *>(kern), smem);
     kern<<<count, kNodeThreads, smem, s>>>(tasks, form, max_s, max_r, stage, info);
   };
   if (max_s <= 32) go(node_factor_kernel<TW, TE, 1>);

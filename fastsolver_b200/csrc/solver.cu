@@ -50,6 +50,7 @@ struct PathSpec {
   int ob = 0;                            // leaf outer block width (0: one level)
   bool factor = false;
   int red_chunk = 512, bc_chunk = 512;
+  int leaf_size = 1;  // nodes with at most this many real leaves use the 2r x 2r form
 };
 
 // Rows per split-K slot of a child with `nrow` rows: at least `chunk` rows,
@@ -349,7 +350,7 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
     auto L = std::make_unique<LevelPlan<T, TE>>();
     std::vector<GemmItem<T, T>> ri, bi;
     std::vector<GemmSeg<T>> rs, bs;
-    std::vector<NodeTask<T, TE>> nt;
+    std::vector<NodeTask<T, TE>> nt[2];
     std::vector<SumTask<T>> su;
     std::vector<GemmItem<T, double>> gi;
     std::vector<GemmSeg<T>> gs;
@@ -424,8 +425,10 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
       k.F = sp.ns->F.p + (size_t)p * sp.ns->rr;
       k.M = sp.M + (size_t)p * sp.ns->mm;
       k.info_slot = nleaf + p;
-      nt.push_back(k);
-      if (sp.factor && form == 0) {
+      // the node's form: 1 everywhere when asked for, else 1 inside a Legion leaf
+      const int nform = (form == 1 || inside_legion_leaf(t, p, sp.leaf_size)) ? 1 : 0;
+      nt[nform].push_back(k);
+      if (sp.factor && nform == 0) {
         // S = I - V1Tu1 V0Tu0 (r0 x r0, ld r0): the dgemm at solver_tasks.cc:261
         GemmSeg<T> g{};
         g.A = k.W1u;
@@ -445,9 +448,9 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
         gi.push_back(it);
         L->gram_max = std::max(L->gram_max, r0);
       }
-      const int s = form == 0 ? r0 : s2;
-      L->max_s = std::max(L->max_s, s);
-      L->max_r = std::max(L->max_r, std::max(r0, r1));
+      const int s = nform == 0 ? r0 : s2;
+      L->max_s[nform] = std::max(L->max_s[nform], s);
+      L->max_r[nform] = std::max(L->max_r[nform], std::max(r0, r1));
       if (cw > 0) {
         // [eta0; eta1] = M [V0Td0; V1Td1]: one item, two K segments
         GemmSeg<T> a0{}, a1{};
@@ -510,8 +513,10 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
     L->gram_items.upload(gi);
     L->gram_segs.upload(gs);
     L->n_gram = (int)gi.size();
-    L->node_tasks.upload(nt);
-    L->n_nodes = (int)nt.size();
+    for (int f = 0; f < 2; ++f) {
+      L->node_tasks[f].upload(nt[f]);
+      L->n_nodes[f] = (int)nt[f].size();
+    }
     L->ap_items.upload(ai);
     L->ap_segs.upload(as);
     L->n_ap = (int)ai.size();
@@ -614,10 +619,13 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
     }
     if (plan.factor) {
       PhaseScope ps(pf, PH_NODE_FACTOR, s);
-      if (form == 0)
+      if (L.n_gram > 0)
         launch_gemm_items<T, double, double>(L.gram_items.p, L.gram_segs.p, L.n_gram, L.gram_max,
                                              L.gram_max, false, -1.0, 1.0, s);
-      launch_node_factor<T, TE>(L.node_tasks.p, L.n_nodes, L.max_s, L.max_r, form, info, s);
+      for (int f = 0; f < 2; ++f)
+        if (L.n_nodes[f] > 0)
+          launch_node_factor<T, TE>(L.node_tasks[f].p, L.n_nodes[f], L.max_s[f], L.max_r[f], f,
+                                    info, s);
     }
     {
       PhaseScope ps(pf, PH_NODE_APPLY, s);
@@ -882,7 +890,7 @@ void merge_paths(const std::vector<const PathPlan<T, TE> *> &src, const std::vec
     ItemAcc<T, T> red, ap, bc;
     ItemAcc<T, double> gram;
     std::vector<SumTask<T>> su;
-    std::vector<NodeTask<T, TE>> nt;
+    std::vector<NodeTask<T, TE>> nt[2];
     for (size_t k = 0; k < src.size(); ++k) {
       if (j >= src[k]->levels.size()) continue;
       const LevelPlan<T, TE> &S = *src[k]->levels[j];
@@ -892,12 +900,14 @@ void merge_paths(const std::vector<const PathPlan<T, TE> *> &src, const std::vec
       bc.add(S.bc_items.h, S.bc_segs.h);
       su.insert(su.end(), S.sums.h.begin(), S.sums.h.end());
       L->sum_max_len = std::max(L->sum_max_len, S.sum_max_len);
-      for (NodeTask<T, TE> t : S.node_tasks.h) {
-        t.info_slot += info_off[k];
-        nt.push_back(t);
+      for (int f = 0; f < 2; ++f) {
+        for (NodeTask<T, TE> t : S.node_tasks[f].h) {
+          t.info_slot += info_off[k];
+          nt[f].push_back(t);
+        }
+        L->max_s[f] = std::max(L->max_s[f], S.max_s[f]);
+        L->max_r[f] = std::max(L->max_r[f], S.max_r[f]);
       }
-      L->max_s = std::max(L->max_s, S.max_s);
-      L->max_r = std::max(L->max_r, S.max_r);
     }
     red.store(L->red_items, L->red_segs, L->n_red, L->red_max_m, L->red_max_n);
     int gm = 0, gn = 0;
@@ -907,8 +917,10 @@ void merge_paths(const std::vector<const PathPlan<T, TE> *> &src, const std::vec
     bc.store(L->bc_items, L->bc_segs, L->n_bc, L->bc_max_m, L->bc_max_n);
     L->sums.upload(su);
     L->n_sums = (int)su.size();
-    L->node_tasks.upload(nt);
-    L->n_nodes = (int)nt.size();
+    for (int f = 0; f < 2; ++f) {
+      L->node_tasks[f].upload(nt[f]);
+      L->n_nodes[f] = (int)nt[f].size();
+    }
     dst.levels.push_back(std::move(L));
   }
   dst.built = true;
@@ -1026,6 +1038,7 @@ void System::ensure_fp64() {
     f.D = DLU64.p; f.ldd = N; f.ipiv = ipiv64.p; f.perm = perm64.p;
     f.V = V.p; f.ldv = N; f.part = part64.p; f.wfin = wfin64.p; f.eta = eta64.p; f.M = ns64.M64.p; f.ns = &ns64;
     f.factor = true; f.red_chunk = red_chunk; f.bc_chunk = bc_chunk; f.ob = ob64;
+    f.leaf_size = leaf_size;
     build_path(tree, f, fused64[form], form);
     PathSpec<double, double> a = f;
     a.X = Y64.p; a.factor = false; a.factors = &fused64[form].leaf;

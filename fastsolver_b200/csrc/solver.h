@@ -68,8 +68,10 @@ struct LevelPlan {
   DevBuf<GemmItem<T, double>> gram_items;  // S = I - V1Tu1 V0Tu0, FP64 result
   DevBuf<GemmSeg<T>> gram_segs;
   int n_gram = 0, gram_max = 0;
-  DevBuf<NodeTask<T, TE>> node_tasks;
-  int n_nodes = 0, max_s = 0, max_r = 0;
+  // node factorization tasks by form (0: r x r reduced system, 1: 2r x 2r
+  // permuted Schur system of the nodes inside a Legion leaf)
+  DevBuf<NodeTask<T, TE>> node_tasks[2];
+  int n_nodes[2] = {0, 0}, max_s[2] = {0, 0}, max_r[2] = {0, 0};
   DevBuf<GemmItem<T, T>> ap_items;  // [eta0; eta1] = M [V0Td0; V1Td1] per node
   DevBuf<GemmSeg<T>> ap_segs;
   int n_ap = 0, ap_max_m = 0, ap_max_n = 0;
@@ -253,6 +255,9 @@ struct System {
   int ob32 = 128, ob64 = 0;  // leaf outer block width per path (0: one level)
   int bc_chunk = 512;
   int n_info = 0;
+  // granularity of the reference's tasks (HodlrMatrix leafSize): the FP64
+  // fused path solves the nodes inside a Legion leaf with the 2r x 2r form
+  int leaf_size = 1;
   Profiler prof;
   bool use_graphs = true;  // replay captured segments (off while profiling)
   GraphSeg g_factor32, g_sweep32, g_factor64, g_fused64[2], g_sweep64;
@@ -330,3 +335,11 @@ struct Batch {
 };
 
 }  // namespace hodlr
+
+// The C ABI's opaque handles (include/hodlr_gpu.h).
+struct hodlr_system_s {
+  hodlr::System sys;
+};
+struct hodlr_batch_s {
+  hodlr::Batch b;
+};

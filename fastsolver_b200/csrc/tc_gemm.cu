@@ -36,6 +36,12 @@
 namespace hodlr {
 
 __device__ int g_tc_error = 0;
+// Test hooks of the timeout path (hodlr_debug_tc_wait_hook): the bound of
+// every mbarrier wait, and a one-shot request that the MMA issuer of CTA 0
+// leave out the completion signal of its first tile, so that the epilogue's
+// bounded wait for that tile runs out and the kernel takes its error exit.
+__device__ long long g_tc_spin_limit = 1LL << 22;
+__device__ int g_tc_skip_commit = 0;
 
 namespace {
 
@@ -53,9 +59,9 @@ constexpr int BK = 64 / ELEM;        // K per stage
 constexpr int MMA_K = 32 / ELEM;     // K per tcgen05.mma
 // Bounded mbarrier waits: each try_wait may suspend the thread for up to
 // kSuspendNs (it returns as soon as the phase completes), so waiting warps
-// do not take issue slots from the working ones; kSpinLimit tries bound the
-// wait to a few seconds before the kernel gives up.
-constexpr long long kSpinLimit = 1LL << 22;
+// do not take issue slots from the working ones; g_tc_spin_limit tries
+// (2^22 by default, a few seconds) bound a wait before the kernel gives up.
+constexpr long long kSpinLimitDefault = 1LL << 22;
 constexpr unsigned kSuspendNs = 1000;
 
 __device__ inline uint32_t smem_u32(const void *p) {
@@ -67,9 +73,9 @@ __device__ inline void mbar_init(uint64_t *bar, uint32_t count) {
 }
 
 // Bounded wait for the completion of phase `parity`; false on timeout.
-__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity) {
+__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
   const uint32_t a = smem_u32(bar);
-  for (long long it = 0; it < kSpinLimit; ++it) {
+  for (long long it = 0; it < limit; ++it) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -327,6 +333,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
   __shared__ volatile int abort_sh;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int total = nitems * mtiles * ntn;
+  const long long spin_limit = g_tc_spin_limit > 0 ? g_tc_spin_limit : kSpinLimitDefault;
 
   if (tid == 0) {
     for (int s = 0; s < kStagesP; ++s) {
@@ -484,7 +491,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
         }
       }
       cslot = (cslot + 1) % kStg;
-      if (!mbar_wait(&empty[stage], phase ^ 1)) {
+      if (!mbar_wait(&empty[stage], phase ^ 1, spin_limit)) {
         abort_sh = 1;
         if (!colmode) break;
         continue;  // the group leaves together at the next vote
@@ -511,19 +518,21 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       const uint32_t idesc = instr_desc(BM, BN);
       int stage = 0, acc = 0;
       uint32_t phase = 0, aphase = 0;
+      // test hook: leave out the first tile's completion signal (one launch)
+      bool skip_commit = blockIdx.x == 0 && atomicExch(&g_tc_skip_commit, 0) != 0;
       for (int t = blockIdx.x; t < total && !abort_sh; t += gridDim.x) {
         GemmItem<float, TC> it;
         int m0, n0, Mu, Nu;
         if (!decode(t, it, m0, n0, Mu, Nu)) continue;
         // the epilogue has drained this accumulator and preloaded it with
         // (beta / alpha) Cin when the item has one
-        if (!mbar_wait(&tready[acc], aphase)) { abort_sh = 1; break; }
+        if (!mbar_wait(&tready[acc], aphase, spin_limit)) { abort_sh = 1; break; }
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(acc * BN);
         const int nst = kstages(it);
         const uint32_t pre = (it.Cin != nullptr && beta != 0.f) ? 1u : 0u;
         for (int ks_all = 0; ks_all < nst; ++ks_all) {
-          if (!mbar_wait(&full[stage], phase)) { abort_sh = 1; break; }
+          if (!mbar_wait(&full[stage], phase, spin_limit)) { abort_sh = 1; break; }
           tc_fence_after();
           const uint32_t a_hi = smem_u32(ring + stage * STAGE_BYTES), a_lo = a_hi + A_BYTES;
           const uint32_t b_hi = a_hi + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
@@ -540,11 +549,12 @@ __global__ void __launch_bounds__(kThreadsP, 1)
           if (++stage == kStagesP) { stage = 0; phase ^= 1; }
         }
         if (abort_sh) break;
-        mma_commit(&tfull[acc]);
+        if (skip_commit) skip_commit = false;
+        else mma_commit(&tfull[acc]);
         if (++acc == 2) { acc = 0; aphase ^= 1; }
       }
       mma_commit(&fin);  // all MMAs of this CTA complete before TMEM is freed
-      if (!mbar_wait(&fin, 0)) abort_sh = 1;
+      if (!mbar_wait(&fin, 0, spin_limit)) abort_sh = 1;
     }
   } else {
     // ------------------------------------------------------------ epilogue
@@ -701,7 +711,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       const GemmItem<float, TC> &it = cur.it;
       const int m0 = cur.m0, n0 = cur.n0, Mu = cur.Mu, Nu = cur.Nu;
       const bool live = kstages(it) > 0 || (it.Cin != nullptr && beta != 0.f);
-      const bool ok = mbar_wait(&tfull[acc], aphase);
+      const bool ok = mbar_wait(&tfull[acc], aphase, spin_limit);
       cpa_wait<0>();  // tile j + 2's Cin staged by this thread
       // one barrier: every thread's copies visible, one exit decision for all
       if (epi_vote_or(!ok || abort_sh)) {
@@ -779,8 +789,7 @@ void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int
   constexpr int STG_BYTES = 2 * 128 * BK * 4;
   const size_t smem = (size_t)kStagesP * STAGE_BYTES + (size_t)kStg * STG_BYTES +
                       (size_t)(BN + 4) * 128 * 4 + 128;
-  HODLR_CUDA_TRY(cudaFuncSetAttribute(tc_gemm_persistent<BN, SWAP, TC>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit(reinterpret_cast<const void *>(tc_gemm_persistent<BN, SWAP, TC>), smem);
   const int mt = cdiv(mu_max, BM), nt = cdiv(nu_max, BN);
   const long long total = (long long)nitems * mt * nt;
   int sms = 148;
@@ -832,6 +841,13 @@ int tc_error_flag(bool reset) {
     cudaMemcpyToSymbol(g_tc_error, &z, sizeof(int));
   }
   return h;
+}
+
+void tc_set_wait_hook(long long polls, int skip_one_commit) {
+  const long long lim = polls > 0 ? polls : kSpinLimitDefault;
+  const int skip = skip_one_commit ? 1 : 0;
+  HODLR_CUDA_TRY(cudaMemcpyToSymbol(g_tc_spin_limit, &lim, sizeof(lim)));
+  HODLR_CUDA_TRY(cudaMemcpyToSymbol(g_tc_skip_commit, &skip, sizeof(skip)));
 }
 
 template void launch_tc_gemm<float>(const GemmItem<float, float> *, const GemmSeg<float> *, int,

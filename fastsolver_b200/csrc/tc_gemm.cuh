@@ -15,4 +15,11 @@ void launch_tc_gemm(const GemmItem<float, TC> *items, const GemmSeg<float> *segs
 // (1), 0 if clear, -1 if it could not be read.
 int tc_error_flag(bool reset);
 
+// Test hook of the timeout path: every bounded wait of the engine gives up
+// after `polls` tries (<= 0: the default, 2^22), and with skip_one_commit the
+// next engine launch leaves out one completion signal, so one of its waits
+// runs out; the kernel then raises the error flag, frees its tensor memory
+// and returns.  Synchronous.
+void tc_set_wait_hook(long long polls, int skip_one_commit);
+
 }  // namespace hodlr

@@ -77,19 +77,25 @@ class HodlrMatrix:
 
     Mirrors HodlrMatrix(col, row, gl, sl, r, t, leaf, name): ``rhs_cols``
     right-hand sides, ``rhs_rows`` unknowns, ``rank`` at every level, dense
-    leaves of at most ``threshold`` rows.  Only leafSize == 1 and the
-    single-launch tree (gl == sl) are supported.
+    leaves of at most ``threshold`` rows, ``leaf_size`` real leaves per
+    Legion leaf (the reference's task granularity: it decides the drand48
+    reseeding of init_rhs, the blocks of the text files and, for the FP64
+    fused solve, which nodes use the 2r x 2r leaf-internal form).  The
+    two-level launch (gl != sl) is the multi-GPU subtree split of
+    fastsolver_b200.shard.
     """
 
     def __init__(self, rhs_cols: int, rhs_rows: int, rank: int, threshold: int,
                  leaf_size: int = 1, name: str = "global", glo_level: int | None = None,
                  sub_level: int | None = None):
-        if leaf_size != 1:
-            raise NotImplementedError("leafSize > 1 (several real leaves per task)")
+        if int(leaf_size) < 1:
+            raise ValueError("leaf_size must be >= 1")
         if glo_level is not None and sub_level is not None and glo_level != sub_level:
-            raise NotImplementedError("two-level launch (gloLevel != subLevel)")
+            raise NotImplementedError("two-level launch (gloLevel != subLevel): use "
+                                      "fastsolver_b200.shard for the subtree split")
         self.rhs_cols, self.rhs_rows = int(rhs_cols), int(rhs_rows)
         self.rank, self.threshold = int(rank), int(threshold)
+        self.leaf_size = int(leaf_size)
         self.file_rhs = name + "_rhs.txt"
         self.file_soln = name + "_soln.txt"
         self._h = None
@@ -106,6 +112,8 @@ class HodlrMatrix:
              ctypes.byref(nc), ctypes.byref(ml))
         self.nnodes, self.max_depth, self.nleaves = n.value, d.value, nl.value
         self.ncols, self.max_leaf = nc.value, ml.value
+        if self.leaf_size != 1:
+            call("hodlr_set_leaf_size", self._h, self.leaf_size)
         return self
 
     @property
@@ -120,7 +128,17 @@ class HodlrMatrix:
         return np.frombuffer(buf, dtype=np.int32).reshape(self.nnodes, -1).copy()
 
     def get_num_leaf(self) -> int:
-        return self.nleaves
+        """Legion leaves (tasks); equals the real leaves when leaf_size == 1."""
+        n = lib.hodlr_get_num_leaf(self.handle)
+        check("hodlr_get_num_leaf", min(n, 0))
+        return n
+
+    def legion_leaves(self) -> np.ndarray:
+        """Node ids of the Legion leaves, left to right."""
+        n = lib.hodlr_legion_leaves(self.handle, None, 0)
+        buf = (ctypes.c_int * max(n, 1))()
+        check("hodlr_legion_leaves", min(lib.hodlr_legion_leaves(self.handle, buf, n), 0))
+        return np.array(buf[:n], dtype=np.int32)
 
     def get_num_rhs(self) -> int:
         return self.rhs_cols
@@ -224,41 +242,23 @@ class HodlrMatrix:
         call("hodlr_phase_times", self.handle, ms, ln, int(reset))
         return {k: (ms[i], int(ln[i])) for i, k in enumerate(_lib.PHASES)}
 
-    # -- reference text output (save_region_task.cc:37-67) --------------------
-    def _save(self, filename: str, X: np.ndarray, print_seed: bool):
-        t = self.tree_nodes()
-        leaves = [i for i in range(t.shape[0]) if t[i, 9]]
-        # in-order leaf sequence of the tree (save_HodlrMatrix recursion)
-        order = []
-
-        def walk(i):
-            if t[i, 9]:
-                order.append(i)
-                return
-            walk(t[i, 4])
-            walk(t[i, 5])
-
-        walk(0)
-        assert len(order) == len(leaves)
-        with open(filename, "a") as f:
-            for i in order:
-                rb, n = int(t[i, 2]), int(t[i, 0])
-                if print_seed:
-                    f.write(f"{self._seed}\n")
-                for row in X[rb:rb + n]:
-                    f.write("".join(f"{v:.20g}\t" for v in row) + "\n")
-
+    # -- reference text format (save_region_task.cc:37-67) -------------------
     def save_solution(self, filename: str | None = None):
-        fn = filename or self.file_soln
-        if os.path.exists(fn):
-            os.remove(fn)
-        self._save(fn, self.solution(), False)
+        """HodlrMatrix::save_solution (hodlr_matrix.cc:581-590)."""
+        call("hodlr_save_solution", self.handle, (filename or self.file_soln).encode())
 
-    def save_rhs(self, B: np.ndarray, filename: str | None = None):
-        fn = filename or self.file_rhs
-        if os.path.exists(fn):
-            os.remove(fn)
-        self._save(fn, np.asarray(B), True)
+    def save_rhs(self, filename: str | None = None, seed: int | None = None):
+        """HodlrMatrix::save_rhs (hodlr_matrix.cc:569-579): one seed line per Legion leaf."""
+        sd = self._seed if seed is None else int(seed)
+        call("hodlr_save_rhs", self.handle, (filename or self.file_rhs).encode(), sd)
+
+    def load_rhs(self, filename: str | None = None) -> int:
+        """Read a right-hand-side file in save_rhs's format into b; returns its seed."""
+        sd = ctypes.c_long()
+        call("hodlr_load_rhs", self.handle, (filename or self.file_rhs).encode(),
+             ctypes.byref(sd))
+        self._seed = int(sd.value)
+        return self._seed
 
     def close(self):
         if self._h is not None:
@@ -402,3 +402,33 @@ def node_lu_solve(V0Tu0, V1Tu1, V0Td0, V1Td1, info=None, stream=None) -> int:
 
 def node_schur2_solve(V0Tu0, V1Tu1, V0Td0, V1Td1, info=None, stream=None) -> int:
     return _node("hodlr_node_schur2_solve", V0Tu0, V1Tu1, V0Td0, V1Td1, info, stream)
+
+
+def write_text(filename: str, X, col_beg: int = 0, ncol: int | None = None, seed: int = 0,
+               print_seed: bool = False):
+    """Append X's rows (columns col_beg.. of a 2-D array) in the reference's
+    text format (save_data, save_region_task.cc:37-67)."""
+    A = np.asfortranarray(np.asarray(X, dtype=np.float64))
+    nrow, cols = A.shape
+    ncol = cols - col_beg if ncol is None else int(ncol)
+    call("hodlr_text_write", filename.encode(), A.ctypes.data, max(nrow, 1), nrow,
+         int(col_beg), ncol, int(seed), int(bool(print_seed)))
+
+
+def read_text(filename: str, nrow: int, ncol: int, block_rows=None):
+    """Read an nrow x ncol block written in the reference's text format.
+
+    Without ``block_rows`` the file holds the values only (a solution file,
+    read as direct_solve.cc:201-213 does); with it, one seed line precedes
+    each block of block_rows[b] rows (a right-hand-side file).  Returns
+    (X, seeds)."""
+    X = np.zeros((nrow, ncol), dtype=np.float64, order="F")
+    if block_rows is None:
+        call("hodlr_text_read", filename.encode(), X.ctypes.data, max(nrow, 1), nrow, ncol, 0,
+             None, None)
+        return X, []
+    br = (ctypes.c_int * len(block_rows))(*[int(b) for b in block_rows])
+    sd = (ctypes.c_long * max(len(block_rows), 1))()
+    call("hodlr_text_read", filename.encode(), X.ctypes.data, max(nrow, 1), nrow, ncol,
+         len(block_rows), br, sd)
+    return X, [int(v) for v in sd[:len(block_rows)]]

@@ -38,6 +38,7 @@ typedef void *hodlr_stream_t; /* cudaStream_t */
 #define HODLR_ERR_NOCONV (-1003)   /* refinement did not reach the tolerance */
 #define HODLR_ERR_TIMEOUT (-1004)  /* a bounded device wait gave up */
 #define HODLR_ERR_UNSUPPORTED (-1005)
+#define HODLR_ERR_IO (-1006)       /* text file could not be opened / parsed */
 
 #define HODLR_PREC_FP64 0  /* FP64 throughout (the reference's arithmetic) */
 #define HODLR_PREC_MIXED 1 /* FP32 leaf LU + split-BF16 tensor-core GEMMs,
@@ -142,6 +143,19 @@ int hodlr_gemm_f32(int transa, int m, int n, int k, float alpha, const float *A,
                    int lda, const float *B, int ldb, float beta, float *C,
                    int ldc, int engine, hodlr_stream_t stream);
 
+/* Test hook of the timeout path of the tensor-core engine (no reference
+ * counterpart: the reference has no device waits).  Every bounded mbarrier
+ * wait of the engine gives up after `polls` tries (<= 0 restores the default,
+ * 2^22, a few seconds), and with skip_one_commit != 0 the next engine launch
+ * leaves out the completion signal of one tile, so one of its waits runs out:
+ * the kernel then raises the device error flag, waits (bounded) for its own
+ * tensor-core work, frees its tensor memory and returns.  Every call that
+ * synchronizes (hodlr_factor, hodlr_solve_fused with sync, the refined and
+ * batched solves, hodlr_gemm_f32) reads and clears the flag and returns
+ * HODLR_ERR_TIMEOUT when it was raised; calls that only enqueue work leave it
+ * for the next synchronizing call.  Synchronizes the device. */
+int hodlr_debug_tc_wait_hook(long long polls, int skip_one_commit);
+
 /* ------------------------------------------------------------------------ */
 /* Handle API: the solver that walks the tree (FastSolver + HodlrMatrix)     */
 /* ------------------------------------------------------------------------ */
@@ -233,6 +247,51 @@ int hodlr_relres(hodlr_system sys, double *relres, hodlr_stream_t stream);
 /* Copy the solution (N x m) out: host != 0 -> host memory. */
 int hodlr_get_solution(hodlr_system sys, double *X, long long ldx, int host,
                        hodlr_stream_t stream);
+
+/* Task granularity of the reference (HodlrMatrix's leafSize argument,
+ * src/htree/hodlr_matrix.cc:22-33, 317-337): a Legion leaf is a topmost node
+ * whose subtree holds at most leaf_size real leaves (default 1: the real
+ * leaves).  It decides (a) the drand48 right-hand side, one stream reseeded
+ * per Legion leaf (init_rhs, hodlr_matrix.cc:175-209); (b) the blocks of the
+ * text files (one seed line per Legion leaf, hodlr_matrix.cc:569-605); (c) the
+ * node form of the FP64 fused solve: internal nodes inside a Legion leaf use
+ * the 2r x 2r form of serial_leaf_solve's internal branch
+ * (solver_tasks.cc:452-549), the others LUSolveTask's r x r form.  leaf_size
+ * > 1 needs 2r <= 144 (HODLR_ERR_UNSUPPORTED otherwise).  Discards the FP64
+ * factorization. */
+int hodlr_set_leaf_size(hodlr_system sys, int leaf_size);
+/* Number of Legion leaves (HodlrMatrix::get_num_leaf); the reference's
+ * counter also counts the nodes below a Legion leaf when leafSize > 1, this
+ * returns the data blocks (tasks) only. */
+int hodlr_get_num_leaf(hodlr_system sys);
+/* Node ids (BFS numbering, as hodlr_tree_nodes) of the Legion leaves, left to
+ * right, into ids (cap entries; NULL: count only).  Returns the count. */
+int hodlr_legion_leaves(hodlr_system sys, int *ids, int cap);
+
+/* ---- The reference's text format (src/legion_matrix/save_region_task.cc:
+ * 37-67): every row of a block on its own line, each value printed with 20
+ * significant digits ("%.20g") and followed by a tab, blocks appended to the
+ * file, an optional seed line in front of a block.  Host memory. */
+/* Append rows 0..nrow-1, columns col_beg..col_beg+ncol-1 of the column-major
+ * X (ldx) to `filename`, after a seed line if print_seed (save_data). */
+int hodlr_text_write(const char *filename, const double *X, long long ldx,
+                     int nrow, int col_beg, int ncol, long seed, int print_seed);
+/* Read nrow x ncol values row by row (whitespace separated, as the dense check
+ * reads the solution file, src/solver/direct_solve.cc:201-213) into X (ldx).
+ * With nblocks > 0 the file holds nblocks blocks of block_rows[b] rows (sum =
+ * nrow), each after a seed line; the seeds go to `seeds` (may be NULL).
+ * Returns 0, an argument error or HODLR_ERR_IO (missing file, short or
+ * malformed data). */
+int hodlr_text_read(const char *filename, double *X, long long ldx, int nrow,
+                    int ncol, int nblocks, const int *block_rows, long *seeds);
+/* HodlrMatrix::save_rhs / save_solution (hodlr_matrix.cc:569-605): remove the
+ * file, then write every Legion leaf's rows of b (with `seed` in front of each
+ * block) or of the solution.  hodlr_load_rhs reads a file save_rhs wrote
+ * (for the system's Legion leaves) into b; *seed (may be NULL) receives the
+ * first block's seed.  Synchronous. */
+int hodlr_save_rhs(hodlr_system sys, const char *filename, long seed);
+int hodlr_save_solution(hodlr_system sys, const char *filename);
+int hodlr_load_rhs(hodlr_system sys, const char *filename, long *seed);
 
 /* Per-phase device time.  While profiling is on (off by default), every
  * launch group is bracketed by CUDA events; hodlr_phase_times synchronizes

@@ -321,9 +321,12 @@ static void broadcast_subtree(const int *t, int child, int *leafbuf,
   }
 }
 
-/* fast_solver.cc:191-255 `visit` for an internal node. */
+/* fast_solver.cc:191-255 `visit` for an internal node; inside a Legion leaf
+ * (at most leaf_size real leaves below, mark_legion_leaf at
+ * hodlr_matrix.cc:317-337) the node is solved by serial_leaf_solve's internal
+ * branch (solver_tasks.cc:452-549) with the 2r x 2r form. */
 static int visit_internal(const int *t, int nn, int i, double *X, int ldx,
-                          const double *V, int ldv, int m, int schur2) {
+                          const double *V, int ldv, int m, int schur2, int leaf_size) {
   const int *p = ND(t, i);
   const int *b0 = ND(t, p[F_LCHILD]);
   const int *b1 = ND(t, p[F_RCHILD]);
@@ -332,6 +335,7 @@ static int visit_internal(const int *t, int nn, int i, double *X, int ldx,
   int c0 = b0[F_COLBEG], c1 = b1[F_COLBEG];
   int c = c0; /* rd0 = rd1 = [0, col_beg) */
   int *leafbuf = (int *)malloc(sizeof(int) * (size_t)nn);
+  if (!schur2 && collect_leaves(t, i, leafbuf, 0) <= leaf_size) schur2 = 1;
   double *V0Tu0 = (double *)malloc(sizeof(double) * (size_t)v0c * r0);
   double *V1Tu1 = (double *)malloc(sizeof(double) * (size_t)v1c * r1);
   double *V0Td0 = (double *)malloc(sizeof(double) * (size_t)v0c * (c > 0 ? c : 1));
@@ -366,8 +370,20 @@ static int visit_internal(const int *t, int nn, int i, double *X, int ldx,
  * factors, X[:, 0:m] with the solution.  schur2 != 0 uses the 2r x 2r node
  * form instead of LUSolveTask's r x r form.  Returns 0 or the first nonzero
  * INFO (leaf: its value; node: 100000 + value). */
+int ref_bfs_solve_ls(const int *t, int nn, double *X, int ldx, const double *V,
+                     int ldv, double *D, int ldd, int nthreads, int schur2,
+                     int leaf_size);
+
 int ref_bfs_solve(const int *t, int nn, double *X, int ldx, const double *V,
                   int ldv, double *D, int ldd, int nthreads, int schur2) {
+  return ref_bfs_solve_ls(t, nn, X, ldx, V, ldv, D, ldd, nthreads, schur2, 1);
+}
+
+/* ref_bfs_solve with the reference's task granularity leafSize (the nodes
+ * inside a Legion leaf take the 2r x 2r form). */
+int ref_bfs_solve_ls(const int *t, int nn, double *X, int ldx, const double *V,
+                     int ldv, double *D, int ldd, int nthreads, int schur2,
+                     int leaf_size) {
   int m = t[F_NCOL];
   int maxd = 0;
   for (int i = 0; i < nn; ++i) if (ND(t, i)[F_DEPTH] > maxd) maxd = ND(t, i)[F_DEPTH];
@@ -389,7 +405,7 @@ int ref_bfs_solve(const int *t, int nn, double *X, int ldx, const double *V,
         info = ref_leaf_solve(p[F_NROW], p[F_COLBEG] + p[F_NCOL], D + rb, ldd,
                               X + rb, ldx, 0);
       } else {
-        info = visit_internal(t, nn, i, X, ldx, V, ldv, m, schur2);
+        info = visit_internal(t, nn, i, X, ldx, V, ldv, m, schur2, leaf_size);
         if (info) info += 100000;
       }
       if (info) {

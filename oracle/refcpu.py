@@ -82,6 +82,8 @@ def lib():
         fn.argtypes = [ctypes.c_int] * 3 + [_dp, ctypes.c_int] * 4
     L.ref_bfs_solve.argtypes = [_ip, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int,
                                 _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.ref_bfs_solve_ls.argtypes = [_ip, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int,
+                                   _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.ref_hodlr_matvec.argtypes = [_ip, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int,
                                    _dp, ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int,
                                    ctypes.c_int]
@@ -177,8 +179,32 @@ class System:
         return A
 
 
-def kat_system(N=480, nrhs=2, rank=30, threshold=60, diag=1.0e4, seed=1245667) -> System:
-    """The reference's accuracy run (test/single_launch.cc:20-75)."""
+def legion_leaves(tree: np.ndarray, leaf_size: int = 1):
+    """Topmost nodes with at most leaf_size real leaves below, left to right
+    (mark_legion_leaf, hodlr_matrix.cc:317-337)."""
+    def nreal(i):
+        if tree[i, F["is_leaf"]]:
+            return 1
+        return nreal(int(tree[i, F["lchild"]])) + nreal(int(tree[i, F["rchild"]]))
+
+    out = []
+
+    def walk(i):
+        if nreal(i) <= leaf_size:
+            out.append(i)
+            return
+        walk(int(tree[i, F["lchild"]]))
+        walk(int(tree[i, F["rchild"]]))
+
+    walk(0)
+    return out
+
+
+def kat_system(N=480, nrhs=2, rank=30, threshold=60, diag=1.0e4, seed=1245667,
+               leaf_size=1) -> System:
+    """The reference's accuracy run (test/single_launch.cc:20-75); the drand48
+    right-hand side is reseeded per Legion leaf (init_rhs_recursive,
+    hodlr_matrix.cc:191-209)."""
     L = lib()
     tree = build_tree(N, nrhs, rank, threshold)
     C = total_cols(tree)
@@ -192,6 +218,8 @@ def kat_system(N=480, nrhs=2, rank=30, threshold=60, diag=1.0e4, seed=1245667) -
         blk = fmat(n, nmax)
         L.ref_fill_circulant_k(n, rb, rank, diag, _p(blk), n)
         D[rb:rb + n, :] = blk
+    for i in legion_leaves(tree, leaf_size):
+        rb, n = int(tree[i, F["row_beg"]]), int(tree[i, F["nrow"]])
         bb = fmat(n, nrhs)
         L.ref_drand48_fill(seed, n, nrhs, _p(bb), n)
         B[rb:rb + n, :] = bb
@@ -255,16 +283,17 @@ def gaussian_system(N, nrhs, rank, threshold, seed=1245667, offdiag_norm=0.5) ->
 # solves
 # --------------------------------------------------------------------------
 
-def bfs_solve(sysm: System, nthreads: int = 1, schur2: bool = False):
-    """Fused FP64 solve (fast_solver.cc:136-255). Returns (X, D_lu)."""
+def bfs_solve(sysm: System, nthreads: int = 1, schur2: bool = False, leaf_size: int = 1):
+    """Fused FP64 solve (fast_solver.cc:136-255); leaf_size > 1 solves the
+    nodes inside a Legion leaf with the 2r x 2r form. Returns (X, D_lu)."""
     L = lib()
     X = sysm.X0()
     D = np.asfortranarray(sysm.D.copy())
     t = np.ascontiguousarray(sysm.tree, dtype=np.int32)
     L.ref_set_blas_threads(1)
-    rc = L.ref_bfs_solve(t.ctypes.data_as(_ip), t.shape[0], _p(X), X.shape[0],
-                         _p(sysm.V), sysm.V.shape[0], _p(D), D.shape[0], nthreads,
-                         1 if schur2 else 0)
+    rc = L.ref_bfs_solve_ls(t.ctypes.data_as(_ip), t.shape[0], _p(X), X.shape[0],
+                            _p(sysm.V), sysm.V.shape[0], _p(D), D.shape[0], nthreads,
+                            1 if schur2 else 0, int(leaf_size))
     if rc != 0:
         raise RuntimeError(f"ref_bfs_solve INFO={rc}")
     return X, D
