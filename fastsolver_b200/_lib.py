@@ -24,7 +24,7 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 
 PHASES = ["getrf", "getrs", "reduce", "node_factor", "node_apply", "broadcast", "matvec",
-          "convert", "leaf_panel", "leaf_update", "leaf_trsm"]
+          "convert", "leaf_panel", "leaf_update", "leaf_trsm", "sweep_levels"]
 NODE_FIELDS = ["nrow", "ncol", "row_beg", "col_beg", "lchild", "rchild", "parent", "depth",
                "vncol", "is_leaf"]
 
@@ -90,6 +90,7 @@ _SIGS = {
     "hodlr_reset_launch_count": [],
     "hodlr_status_string": [_i],
     "hodlr_debug_tc_wait_hook": [_ll, _i],
+    "hodlr_debug_sweep_barrier_hook": [_ll, _i],
     "hodlr_set_leaf_size": [_vp, _i],
     "hodlr_get_num_leaf": [_vp],
     "hodlr_legion_leaves": [_vp, _ip, _i],

@@ -82,7 +82,11 @@ struct StreamScratch {
 // HODLR_ERR_TIMEOUT if a tensor-core kernel's bounded wait gave up since the
 // flag was last read (the flag is sticky per device until read), else 0.
 // Call after the work has been synchronized.
-int tc_status() { return tc_error_flag(true) > 0 ? HODLR_ERR_TIMEOUT : 0; }
+int tc_status() {
+  const bool tc = tc_error_flag(true) > 0;
+  const bool sw = sweep_error_flag(true) > 0;
+  return (tc || sw) ? HODLR_ERR_TIMEOUT : 0;
+}
 
 int finish_info(int *info_user, int *info_dev, cudaStream_t s) {
   if (info_user) return 0;
@@ -269,6 +273,15 @@ int hodlr_gemm_f32(int transa, int m, int n, int k, float alpha, const float *A,
       launch_gemm_items<float, float, float>(di, ds, 1, m, n, transa != 0, alpha, beta, s, false);
     HODLR_CUDA_TRY(cudaStreamSynchronize(s));
     return tc_status();
+  });
+}
+
+int hodlr_debug_sweep_barrier_hook(long long polls, int skip_one_arrival) {
+  if (int e = device_ok()) return e;
+  return guarded([&]() -> int {
+    HODLR_CUDA_TRY(cudaDeviceSynchronize());
+    sweep_set_wait_hook(polls, skip_one_arrival);
+    return 0;
   });
 }
 

@@ -18,6 +18,7 @@
 #include <cstdlib>
 
 #include "common.cuh"
+#include "gemm_dmma.cuh"
 #include "gemm_simt.cuh"
 #include "gemm_skinny.cuh"
 #include "tc_gemm.cuh"
@@ -440,6 +441,12 @@ void launch_gemm_items(const GemmItem<TA, TC> *items, const GemmSeg<TA> *segs, i
     launch_tc_gemm<float>(reinterpret_cast<const GemmItem<float, float> *>(items),
                           reinterpret_cast<const GemmSeg<float> *>(segs), nitems, max_m, max_n,
                           trans, float(alpha), float(beta), s);
+    return;
+  } else if (std::is_same<TA, double>::value && std::is_same<TC, double>::value &&
+             std::is_same<TACC, double>::value) {
+    launch_dmma_tile(reinterpret_cast<const GemmItem<double, double> *>(items),
+                     reinterpret_cast<const GemmSeg<double> *>(segs), nitems, max_m, max_n,
+                     trans, double(alpha), double(beta), s);
     return;
   } else if (std::is_same<TA, TACC>::value) {
     using T = TACC;

@@ -16,6 +16,7 @@
 // All launch descriptors are built once per system and live on the device,
 // so a solve is a fixed sequence of launches (capturable in a CUDA graph).
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 
@@ -301,6 +302,45 @@ void run_gemm(const GemmLaunch<TA, TC> &g, bool trans, TACC alpha, TACC beta, cu
 template <typename T>
 void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t s);
 
+// The level descriptors of an FP32 apply path for the persistent sweep
+// kernel, when every level's products have at most 32 columns.
+template <typename T, typename TE>
+void build_sweep(PathPlan<T, TE> &plan) {
+  plan.sweep_ok = false;
+  if constexpr (std::is_same<T, float>::value && std::is_same<TE, float>::value) {
+    if (plan.factor || plan.levels.empty()) return;
+    std::vector<SweepLevel> v;
+    int mx = 0;
+    for (const auto &Lp : plan.levels) {
+      const LevelPlan<T, TE> &L = *Lp;
+      if (L.red_max_n > 32 || L.ap_max_n > 32 || L.bc_max_n > 32) return;
+      SweepLevel d{};
+      d.red_items = L.red_items.p;
+      d.red_segs = L.red_segs.p;
+      d.n_red = L.n_red;
+      d.red_mt = cdiv(std::max(L.red_max_m, 1), 64);
+      d.red_nt = cdiv(std::max(L.red_max_n, 1), 16);
+      d.sums = L.sums.p;
+      d.n_sums = L.n_sums;
+      d.sum_units = (int)cdiv<long long>(std::max<long long>(L.sum_max_len, 1), 512);
+      d.ap_items = L.ap_items.p;
+      d.ap_segs = L.ap_segs.p;
+      d.n_ap = L.n_ap;
+      d.ap_rb = cdiv(std::max(L.ap_max_m, 1), 128);
+      d.bc_items = L.bc_items.p;
+      d.bc_segs = L.bc_segs.p;
+      d.n_bc = L.n_bc;
+      d.bc_rb = cdiv(std::max(L.bc_max_m, 1), 128);
+      mx = std::max(mx, std::max(L.ap_max_n, L.bc_max_n));
+      v.push_back(d);
+    }
+    plan.sweep.upload(v);
+    plan.sweep_bar.ensure(2);
+    plan.sweep_max_n = std::max(mx, 1);
+    plan.sweep_ok = true;
+  }
+}
+
 template <typename T, typename TE>
 void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan, int form) {
   plan.levels.clear();
@@ -525,6 +565,7 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
     L->n_bc = (int)bi.size();
     plan.levels.push_back(std::move(L));
   }
+  build_sweep(plan);
   plan.built = true;
 }
 
@@ -608,6 +649,12 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
   } else {
     PhaseScope ps(pf, PH_GETRS, s);
     launch_getrs<T>(plan.leaf_tasks.p, none, plan.nleaf, plan.max_n, plan.max_nrhs, s);
+  }
+  if (!plan.factor && plan.sweep_ok && sweep_persistent_enabled()) {
+    PhaseScope ps(pf, PH_SWEEP_LEVELS, s);
+    launch_sweep_levels(plan.sweep.p, (int)plan.levels.size(), plan.sweep_max_n,
+                        plan.sweep_bar.p, s);
+    return;
   }
   for (const auto &Lp : plan.levels) {
     const LevelPlan<T, TE> &L = *Lp;
@@ -923,6 +970,7 @@ void merge_paths(const std::vector<const PathPlan<T, TE> *> &src, const std::vec
     }
     dst.levels.push_back(std::move(L));
   }
+  build_sweep(dst);
   dst.built = true;
 }
 

@@ -9,6 +9,7 @@
 #include "common.cuh"
 #include "htree.h"
 #include "leaf_blocked.cuh"
+#include "sweep.cuh"
 #include "util.cuh"
 
 namespace hodlr {
@@ -142,6 +143,11 @@ struct PathPlan {
   DevBuf<LeafFactorTask<T>> apply_tasks;  // apply paths: the factors' tasks on X
   int apply_nb = 0, apply_max_n = 0, apply_max_cols = 0;
   std::vector<std::unique_ptr<LevelPlan<T, TE>>> levels;  // deepest first
+  // FP32 apply paths: the levels as one persistent launch (sweep.cu)
+  DevBuf<SweepLevel> sweep;
+  DevBuf<unsigned> sweep_bar;
+  int sweep_max_n = 0;
+  bool sweep_ok = false;
 };
 
 // Matvec plan: y = beta b + alpha (D x + sum_c U_c V_sib^T x_sib).
@@ -161,7 +167,7 @@ struct MatvecPlan {
 // Optional per-phase timing (CUDA events around each launch group).
 enum Phase {
   PH_GETRF = 0, PH_GETRS, PH_REDUCE, PH_NODE_FACTOR, PH_NODE_APPLY, PH_BCAST, PH_MATVEC,
-  PH_CONVERT, PH_LEAF_PANEL, PH_LEAF_UPDATE, PH_LEAF_TRSM, PH_COUNT
+  PH_CONVERT, PH_LEAF_PANEL, PH_LEAF_UPDATE, PH_LEAF_TRSM, PH_SWEEP_LEVELS, PH_COUNT
 };
 struct Profiler {
   bool on = false;

@@ -156,6 +156,14 @@ int hodlr_gemm_f32(int transa, int m, int n, int k, float alpha, const float *A,
  * for the next synchronizing call.  Synchronizes the device. */
 int hodlr_debug_tc_wait_hook(long long polls, int skip_one_commit);
 
+/* The same for the grid barriers of the persistent sweep kernel (the level
+ * walk of the refinement sweeps): every barrier wait gives up after `polls`
+ * tries (<= 0: the default, 2^22), and with skip_one_arrival != 0 one CTA of
+ * the next sweep launch leaves before its first arrival, so the other CTAs'
+ * waits run out; they raise the device flag and leave.  The refined and
+ * batched solves then return HODLR_ERR_TIMEOUT.  Synchronizes the device. */
+int hodlr_debug_sweep_barrier_hook(long long polls, int skip_one_arrival);
+
 /* ------------------------------------------------------------------------ */
 /* Handle API: the solver that walks the tree (FastSolver + HodlrMatrix)     */
 /* ------------------------------------------------------------------------ */
@@ -301,8 +309,11 @@ int hodlr_load_rhs(hodlr_system sys, const char *filename, long *seed);
  * factorization, all of 8-10), 1 getrs (backward leaf solve / leaf apply),
  * 2 reduce, 3 node factor, 4 node apply, 5 broadcast, 6 matvec, 7 precision
  * conversion, 8 leaf panels (panel LU + row interchanges), 9 leaf trailing
- * updates (A22 -= L21 U12), 10 leaf panel solves (U12 = L11^{-1} A12). */
-#define HODLR_PHASES 11
+ * updates (A22 -= L21 U12), 10 leaf panel solves (U12 = L11^{-1} A12),
+ * 11 the persistent level walk of a refinement sweep (reduce, slot sums,
+ * node apply and broadcast of every level in one launch; 2, 4 and 5 then
+ * stay 0 for the sweeps). */
+#define HODLR_PHASES 12
 int hodlr_set_profiling(hodlr_system sys, int on);
 int hodlr_phase_times(hodlr_system sys, double *ms, long long *launches,
                       int reset);

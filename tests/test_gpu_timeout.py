@@ -74,3 +74,32 @@ def test_refined_solve_timeout_reported_then_recovers(fs, oracle, cuda):
     assert rr <= 1e-12
     Xo, _ = oracle.bfs_solve(s, nthreads=8)
     assert relerr(h.solution(stream=st), Xo[:, :m]) < 1e-11
+
+
+def test_sweep_barrier_timeout_reported_then_recovers(fs, oracle, cuda):
+    """The persistent sweep kernel's grid barrier: one CTA leaves before its
+    first arrival, the others' bounded waits run out and the kernel ends; the
+    refined solve reports HODLR_ERR_TIMEOUT and the next one is correct."""
+    import torch
+    from fastsolver_b200._lib import lib
+    from gpu_util import relerr
+    N, m, r, t = 8192, 3, 20, 256
+    s = oracle.gaussian_system(N, m, r, t, seed=23)
+    h = fs.HodlrMatrix(m, N, r, t).create_tree()
+    h.set_matrix(s.D, s.U, s.V)
+    h.set_rhs(s.B)
+    sol = fs.FastSolver()
+    st = torch.cuda.Stream()
+    it, rr = sol.solve_refined(h, fs.PREC_MIXED, tol=1e-12, maxiter=10, stream=st)
+    assert rr <= 1e-12 and it >= 1     # at least one sweep: the kernel ran
+    try:
+        assert lib.hodlr_debug_sweep_barrier_hook(POLLS, 1) == 0
+        with pytest.raises(fs.HodlrError) as e:
+            sol.solve_refined(h, fs.PREC_MIXED, tol=1e-12, maxiter=10, stream=st)
+        assert e.value.status == fs.ERR_TIMEOUT
+    finally:
+        assert lib.hodlr_debug_sweep_barrier_hook(0, 0) == 0
+    it, rr = sol.solve_refined(h, fs.PREC_MIXED, tol=1e-12, maxiter=10, stream=st)
+    assert rr <= 1e-12
+    Xo, _ = oracle.bfs_solve(s, nthreads=8)
+    assert relerr(h.solution(stream=st), Xo[:, :m]) < 1e-11
