@@ -5,9 +5,9 @@
 // blocked LU, the reduce V^T [d | u] of gemm.cc:315-384 and the broadcast
 // d -= u eta of gemm.cc:417-478) runs every wide product through this kernel:
 //   C = beta Cin + alpha sum_s op(A_s) B_s,  op(A) = A (M x K) or A^T (A K x M).
-// One CTA computes a BM x 128 tile of one item (BM = 128 or 64), 8 warps in a
-// 2 x 4 grid, each warp a (BM / 2) x 32 block as (BM / 32) x 4 DMMA tiles of
-// 16 x 8; K advances 16 at a time through a 3-stage cp.async ring (16-byte
+// One CTA computes a BM x 128 tile of one item (BM = 64, two CTAs per SM, or
+// 128 for items of at most 128 rows), 8 warps in a 2 x 4 grid, each warp a
+// (BM / 2) x 32 block as (BM / 32) x 4 DMMA tiles of 16 x 8; K advances 16 at a time through a 3-stage cp.async ring (16-byte
 // copies where the addresses allow, zero fill outside the item).  One DMMA
 // does the work of 512 FP64 FMAs, so the kernel is bound by the FP64 pipe
 // rather than by instruction issue.  Shared-memory layouts (doubles):
@@ -61,17 +61,23 @@ constexpr int a_stage_doubles() {
 constexpr int b_stage_doubles() { return BN * LDK; }
 
 template <int BM, bool TRANS>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, BM == 64 ? 2 : 1)
     gemm_dmma_tile_kernel(const GemmItem<double, double> *__restrict__ items,
-                          const GemmSeg<double> *__restrict__ segs, double alpha, double beta) {
+                          const GemmSeg<double> *__restrict__ segs, double alpha, double beta,
+                          int mtiles, int ntiles) {
   constexpr int MT = BM / 32;          // 16-row DMMA tiles per warp
   constexpr int AP = BM + 4;           // As[k][m] row stride (non-trans)
   constexpr int AS = a_stage_doubles<BM, TRANS>(), BS = b_stage_doubles();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *As = reinterpret_cast<double *>(smem_raw);
   double *Bs = As + (size_t)kStages * AS;
-  const GemmItem<double, double> it = items[blockIdx.x];
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.z * BN;
+  // one-dimensional grid, the tiles of an item consecutive (column tiles
+  // fastest): CTAs resident together share the item's A rows and B columns
+  // through L2
+  const int per = mtiles * ntiles;
+  const int itx = blockIdx.x / per, rem = blockIdx.x - itx * per;
+  const GemmItem<double, double> it = items[itx];
+  const int m0 = (rem / ntiles) * BM, n0 = (rem % ntiles) * BN;
   if (m0 >= it.M || n0 >= it.N) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -242,8 +248,11 @@ void launch_bm(const GemmItem<double, double> *items, const GemmSeg<double> *seg
   const size_t smem =
       (size_t)kStages * (a_stage_doubles<BM, TRANS>() + b_stage_doubles()) * sizeof(double);
   raise_smem_limit(reinterpret_cast<const void *>(gemm_dmma_tile_kernel<BM, TRANS>), smem);
-  dim3 grid(nitems, cdiv(max_m, BM), cdiv(max_n, BN));
-  gemm_dmma_tile_kernel<BM, TRANS><<<grid, kThreads, smem, s>>>(items, segs, alpha, beta);
+  const int mt = cdiv(max_m, BM), nt = cdiv(max_n, BN);
+  const long long total = (long long)nitems * mt * nt;
+  if (total > 0x7fffffffLL) throw CudaError{cudaErrorInvalidConfiguration};
+  gemm_dmma_tile_kernel<BM, TRANS>
+      <<<(unsigned)total, kThreads, smem, s>>>(items, segs, alpha, beta, mt, nt);
   HODLR_LAUNCH_CHECK();
 }
 
@@ -253,12 +262,19 @@ void launch_dmma_tile(const GemmItem<double, double> *items, const GemmSeg<doubl
                       int nitems, int max_m, int max_n, bool trans, double alpha, double beta,
                       cudaStream_t s) {
   if (nitems <= 0 || max_m <= 0 || max_n <= 0) return;
-  if (max_m <= 64) {
-    if (trans) launch_bm<64, true>(items, segs, nitems, max_m, max_n, alpha, beta, s);
-    else launch_bm<64, false>(items, segs, nitems, max_m, max_n, alpha, beta, s);
-  } else {
+  // Items of at most 128 rows run as one tile row of 128: the leaf LU's
+  // block-row solves compute C = L^{-1} C in place (C is also the B operand),
+  // which is only correct when a single CTA reads all of C's rows before it
+  // writes any.  Taller items (the trailing updates, the broadcast) are never
+  // in place and take 64-row tiles: two CTAs per SM, so one CTA's C loads and
+  // stores overlap the other's DMMAs (a 128-row tile needs ~250 registers per
+  // thread and runs alone on its SM).
+  if (max_m > 64 && max_m <= 128) {
     if (trans) launch_bm<128, true>(items, segs, nitems, max_m, max_n, alpha, beta, s);
     else launch_bm<128, false>(items, segs, nitems, max_m, max_n, alpha, beta, s);
+  } else {
+    if (trans) launch_bm<64, true>(items, segs, nitems, max_m, max_n, alpha, beta, s);
+    else launch_bm<64, false>(items, segs, nitems, max_m, max_n, alpha, beta, s);
   }
 }
 

@@ -99,6 +99,43 @@ __device__ inline void node_product(int rows, int cols, int K, double alpha, boo
   }
 }
 
+// The same product with both operands FP64 column-major in shared memory,
+// on the FP64 tensor pipe (mma.m16n8k4.f64): every warp takes 16 x 8 output
+// tiles in turn.  Fragments (g = lane / 4, t = lane % 4): A a0 = A[g][t],
+// a1 = A[g + 8][t]; B b = B[t][g]; C c0..c3 = C[g][2t], C[g][2t + 1],
+// C[g + 8][2t], C[g + 8][2t + 1].  Against the SIMT product it reads a
+// fifth of the shared-memory bytes per multiply-add.
+template <typename FO>
+__device__ inline void node_product_dmma(int rows, int cols, int K, double alpha,
+                                         bool add_identity, const double *A, int lda,
+                                         const double *B, int ldb, FO out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int tm = (rows + 15) / 16, tn = (cols + 7) / 8;
+  for (int tile = warp; tile < tm * tn; tile += kNodeWarps) {
+    const int m0 = (tile / tn) * 16, n0 = (tile % tn) * 8;
+    double c[4] = {0.0, 0.0, 0.0, 0.0};
+    const int ra = m0 + g, rb = m0 + g + 8, cb = n0 + g;
+    for (int k = 0; k < K; k += 4) {
+      const int kk = k + t;
+      const bool kin = kk < K;
+      const double a0 = (kin && ra < rows) ? A[ra + kk * lda] : 0.0;
+      const double a1 = (kin && rb < rows) ? A[rb + kk * lda] : 0.0;
+      const double b = (kin && cb < cols) ? B[kk + cb * ldb] : 0.0;
+      asm volatile(
+          "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, "
+          "{%0, %1, %2, %3};\n"
+          : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+          : "d"(a0), "d"(a1), "d"(b));
+    }
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = m0 + g + (v >> 1) * 8, j = n0 + 2 * t + (v & 1);
+      if (i < rows && j < cols) out(i, j, (add_identity && i == j ? 1.0 : 0.0) + alpha * c[v]);
+    }
+  }
+}
+
 template <typename TW, typename TE, int RL>
 __global__ void __launch_bounds__(kNodeThreads)
     node_factor_kernel(const NodeTask<TW, TE> *tasks, int form, int max_s, int max_r, int stage,
@@ -211,15 +248,26 @@ __global__ void __launch_bounds__(kNodeThreads)
       const int c = lane + 32 * u;
       prow[u] = c < s ? A[p * lda + c] : 0.0;
     }
-    for (int i = warp; i < s; i += kNodeWarps) {
-      if (i == p) continue;
+    // this warp's rows i = warp, warp + kNodeWarps, ...: all multipliers are
+    // read before any lane writes column k (one __syncwarp), so the row
+    // updates are independent and overlap
+    constexpr int RW = (kMaxNodeS + kNodeWarps - 1) / kNodeWarps;
+    double fr[RW];
+#pragma unroll
+    for (int jj = 0; jj < RW; ++jj) {
+      const int i = warp + kNodeWarps * jj;
+      fr[jj] = (i < s && i != p) ? A[i * lda + k] * rinv : 0.0;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int jj = 0; jj < RW; ++jj) {
+      const int i = warp + kNodeWarps * jj;
+      if (i >= s || i == p) continue;
       double *Ai = A + i * lda;
-      const double f = Ai[k] * rinv;
-      __syncwarp();
 #pragma unroll
       for (int u = 0; u < RL; ++u) {
         const int c = lane + 32 * u;
-        if (c < s) Ai[c] = (c == k) ? -f : Ai[c] - f * prow[u];
+        if (c < s) Ai[c] = (c == k) ? -fr[jj] : Ai[c] - fr[jj] * prow[u];
       }
     }
     prevp = p;
@@ -274,24 +322,19 @@ __global__ void __launch_bounds__(kNodeThreads)
     }
     __syncthreads();
     // G0 = -S^{-1} V1Tu1 (r0 x r1): M's upper left block, kept for the last product
-    node_product(
-        r0, r1, r0, -1.0, false, [&](int i, int k) { return Ss[i + k * r0]; },
-        [&](int k, int c) { return W1s[k + c * r0]; },
-        [&](int i, int c, double v) {
-          Gs[i + c * r0] = v;
-          M[i + (long long)c * ldm] = TE(v);
-        });
+    node_product_dmma(r0, r1, r0, -1.0, false, Ss, r0, W1s, r0, [&](int i, int c, double v) {
+      Gs[i + c * r0] = v;
+      M[i + (long long)c * ldm] = TE(v);
+    });
     // -V0Tu0 S^{-1} (r1 x r0): M's lower right block
-    node_product(
-        r1, r0, r0, -1.0, false, [&](int i, int k) { return W0s[i + k * r1]; },
-        [&](int k, int c) { return Ss[k + c * r0]; },
-        [&](int i, int c, double v) { M[(r0 + i) + (long long)(r1 + c) * ldm] = TE(v); });
+    node_product_dmma(r1, r0, r0, -1.0, false, W0s, r1, Ss, r0, [&](int i, int c, double v) {
+      M[(r0 + i) + (long long)(r1 + c) * ldm] = TE(v);
+    });
     __syncthreads();
     // I - V0Tu0 G0 (r1 x r1): M's lower left block
-    node_product(
-        r1, r1, r0, -1.0, true, [&](int i, int k) { return W0s[i + k * r1]; },
-        [&](int k, int c) { return Gs[k + c * r0]; },
-        [&](int i, int c, double v) { M[(r0 + i) + (long long)c * ldm] = TE(v); });
+    node_product_dmma(r1, r1, r0, -1.0, true, W0s, r1, Gs, r0, [&](int i, int c, double v) {
+      M[(r0 + i) + (long long)c * ldm] = TE(v);
+    });
     return;
   }
   const TW *W0u = tk.W0u, *W1u = tk.W1u;

@@ -51,19 +51,26 @@ struct PathSpec {
   int ob = 0;                            // leaf outer block width (0: one level)
   bool factor = false;
   int red_chunk = 512, bc_chunk = 512;
+  int max_slots = 64;  // split-K slots per child at most
   int leaf_size = 1;  // nodes with at most this many real leaves use the 2r x 2r form
 };
 
 // Rows per split-K slot of a child with `nrow` rows: at least `chunk` rows,
-// at most kMaxSlots slots (the node kernels read one summed W per child).
+// at most `max_slots` slots (the slots are summed into one W per child).
+// The factor passes use up to 64 slots of >= 512 rows (wide products, few
+// long tiles per SM); the FP32 refinement sweeps, whose products have only
+// m columns, up to 1024 slots of >= 128 rows, so that the persistent sweep
+// kernel's reduce step has many short units instead of a few long ones.
 constexpr int kMaxSlots = 64;
-inline int slot_rows(int nrow, int chunk) {
-  const int ns = std::max(1, std::min(cdiv(nrow, chunk), kMaxSlots));
+constexpr int kSweepChunk = 128, kSweepMaxSlots = 1024;
+inline int slot_rows(int nrow, int chunk, int max_slots = kMaxSlots) {
+  const int ns = std::max(1, std::min(cdiv(nrow, chunk), max_slots));
   return cdiv(cdiv(nrow, ns), 16) * 16;
 }
 
 // Partial-sum, summed-W and eta workspace (elements) of a path's largest level.
-void path_need(const Tree &t, bool factor, int chunk, size_t &part, size_t &wfin, size_t &eta) {
+void path_need(const Tree &t, bool factor, int chunk, size_t &part, size_t &wfin, size_t &eta,
+               int max_slots = kMaxSlots) {
   part = wfin = eta = 0;
   for (int d = t.max_depth - 1; d >= 0; --d) {
     size_t p = 0, w = 0, e = 0;
@@ -73,7 +80,7 @@ void path_need(const Tree &t, bool factor, int chunk, size_t &part, size_t &wfin
       const int cw = factor ? c0.col_beg : t.nrhs;
       for (const Node *c : {&c0, &c1}) {
         const int NW = factor ? c->col_beg + c->ncol : t.nrhs;
-        const int ns = cdiv(c->nrow, slot_rows(c->nrow, chunk));
+        const int ns = cdiv(c->nrow, slot_rows(c->nrow, chunk, max_slots));
         p += (size_t)ns * c->vncol * NW;
         if (ns > 1) w += (size_t)c->vncol * NW;
       }
@@ -108,7 +115,8 @@ void build_leaf_plan(const Tree &t, T *Dbase, long long ldd, T *Xbase, long long
   lp.Linv.ensure((size_t)nleaf * max_panels * NB * NB);
   lp.Uinv.ensure((size_t)nleaf * max_panels * NB * NB);
   // block-row solves by the inverses of the outer diagonal blocks: in place
-  // on the block's rows, which one GEMM tile row (128) covers
+  // on the block's rows, which one GEMM tile row (128) covers (the GEMM
+  // launchers run launches of items of at most 128 rows as 128-row tiles)
   const bool binv = P > 1 && OB <= 128;
   lp.binv = binv;
   if (binv) {
@@ -322,7 +330,7 @@ void build_sweep(PathPlan<T, TE> &plan) {
       d.red_nt = cdiv(std::max(L.red_max_n, 1), 16);
       d.sums = L.sums.p;
       d.n_sums = L.n_sums;
-      d.sum_units = (int)cdiv<long long>(std::max<long long>(L.sum_max_len, 1), 512);
+      d.sum_units = (int)cdiv<long long>(std::max<long long>(L.sum_max_len, 1), kSweepSumChunk);
       d.ap_items = L.ap_items.p;
       d.ap_segs = L.ap_segs.p;
       d.n_ap = L.n_ap;
@@ -335,7 +343,7 @@ void build_sweep(PathPlan<T, TE> &plan) {
       v.push_back(d);
     }
     plan.sweep.upload(v);
-    plan.sweep_bar.ensure(2);
+    plan.sweep_bar.ensure(kSweepBarWords);
     plan.sweep_max_n = std::max(mx, 1);
     plan.sweep_ok = true;
   }
@@ -408,7 +416,7 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
         const Node &c = side ? c1 : c0;
         const int NW = sp.factor ? c.col_beg + c.ncol : m;
         const int M = c.vncol;
-        const int rows_per = slot_rows(c.nrow, sp.red_chunk);
+        const int rows_per = slot_rows(c.nrow, sp.red_chunk, sp.max_slots);
         const int nslots = cdiv(c.nrow, rows_per);
         T *slot0 = sp.part + poff;
         for (int q = 0; q < nslots; ++q) {
@@ -1106,7 +1114,7 @@ void System::ensure_mixed() {
   alloc_node_store(ns32, tree, false);
   size_t pf, wf, ef, pa, wa, ea;
   path_need(tree, true, red_chunk, pf, wf, ef);
-  path_need(tree, false, red_chunk, pa, wa, ea);
+  path_need(tree, false, kSweepChunk, pa, wa, ea, kSweepMaxSlots);
   part32.ensure(std::max<size_t>(std::max(pf, pa), 1));
   wfin32.ensure(std::max<size_t>(std::max(wf, wa), 1));
   eta32.ensure(std::max<size_t>(std::max(ef, ea), 1));
@@ -1119,6 +1127,8 @@ void System::ensure_mixed() {
   build_path(tree, f, fused32, 0);
   PathSpec<float, float> a = f;
   a.X = Y32.p; a.factor = false; a.factors = &fused32.leaf;
+  a.red_chunk = kSweepChunk;
+  a.max_slots = kSweepMaxSlots;
   build_path(tree, a, apply32, 0);
 }
 

@@ -8,12 +8,13 @@
 // launch per step (four per level) spends most of its time ramping up and
 // draining.  sweep_levels_kernel runs all of them: one cooperative launch of
 // as many 128-thread CTAs as fit on the GPU, every CTA taking work units of a
-// step by grid stride (a 64 x 16 block of a reduce item, 512 elements of a
+// step by grid stride (a 64 x 16 block of a reduce item, 32 elements of a
 // slot sum, 128 rows of an apply or broadcast item -- the same CTA units as
 // the one-step kernels, skinny_units.cuh), and a grid barrier between steps.
 //
-// The grid barrier is a counter in global memory: each CTA adds one and waits
-// until the count reaches (barriers passed) x (CTAs).  Every wait is bounded
+// The grid barrier is a counter in global memory: each CTA adds one, and the
+// CTA whose arrival completes the barrier publishes it in a release word that
+// the others poll with backoff.  Every wait is bounded
 // (g_sweep_spin_limit polls with a sleep); on timeout the CTA raises
 // g_sweep_error and an abort flag, and every CTA leaves at its next barrier,
 // so the kernel always ends.  The host reports the flag as
@@ -41,29 +42,40 @@ namespace {
 using namespace sk;
 constexpr int kThreads = 128;
 constexpr long long kSweepSpinDefault = 1LL << 22;
-constexpr int kSumChunk = 512;  // slot-sum elements per unit (4 per thread)
 
 // Grid barrier; false when the kernel is being abandoned (a wait ran out).
-__device__ bool grid_sync(unsigned *bar, unsigned &target, long long limit) {
+// bar[0] counts arrivals; the CTA whose arrival completes barrier k publishes
+// k + 1 in bar[32] (its own 128-byte line, so the waiting CTAs poll a line
+// that no atomic touches) and bar[64] is the abort flag.  Waiters back off
+// exponentially up to ~1 us between polls, which keeps hundreds of polling
+// CTAs from saturating the L2 slice that holds the flag.
+__device__ bool grid_sync(unsigned *bar, unsigned &gen, long long limit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned *cnt = bar;
-    volatile unsigned *abort = bar + 1;
-    target += gridDim.x;
+    volatile unsigned *release = bar + 32;
+    volatile unsigned *abort = bar + 64;
+    ++gen;
     __threadfence();  // this CTA's results before its arrival
-    atomicAdd(bar, 1u);
+    const unsigned old = atomicAdd(bar, 1u);
     int ok = 1;
-    for (long long it = 0;; ++it) {
-      if (*abort) { ok = 0; break; }
-      if (*cnt >= target) break;
-      if (it >= limit) {
-        atomicExch(bar + 1, 1u);
-        atomicExch(&g_sweep_error, 1);
-        ok = 0;
-        break;
+    if (old == gen * gridDim.x - 1) {
+      __threadfence();
+      *release = gen;  // the last arrival opens the barrier
+    } else {
+      unsigned sleep = 32;
+      for (long long it = 0;; ++it) {
+        if (*release >= gen) break;
+        if (*abort) { ok = 0; break; }
+        if (it >= limit) {
+          atomicExch(bar + 64, 1u);
+          atomicExch(&g_sweep_error, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(sleep);
+        if (sleep < 1024) sleep <<= 1;
       }
-      __nanosleep(128);
     }
     __threadfence();  // the other CTAs' results after the barrier
     s_ok = ok;
@@ -85,7 +97,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     __syncthreads();
     if (s_skip) return;  // test hook: this CTA never arrives
   }
-  unsigned target = 0;
+  unsigned gen = 0;
   const int tid = threadIdx.x;
   for (int l = 0; l < nlevels; ++l) {
     const SweepLevel L = levels[l];
@@ -99,21 +111,29 @@ __global__ void __launch_bounds__(kThreads, 4)
                               rem % L.red_nt, smem);
       }
     }
-    if (!grid_sync(bar, target, limit)) return;
-    // slot sums in a fixed order (the REDOP_ADD of gemm.cc:74-133, deterministic)
+    if (!grid_sync(bar, gen, limit)) return;
+    // slot sums in a fixed order (the REDOP_ADD of gemm.cc:74-133,
+    // deterministic): a unit is 32 elements of one task; warp w adds slots
+    // w, w + 4, ..., then warp 0 adds the four partial sums in order
     {
+      double *part = reinterpret_cast<double *>(smem);  // [4][32]
+      const int lane = tid & 31, w = tid >> 5;
       const int nu = L.n_sums * L.sum_units;
       for (int u = blockIdx.x; u < nu; u += gridDim.x) {
         const SumTask<float> tk = L.sums[u / L.sum_units];
-        const long long e0 = (long long)(u % L.sum_units) * kSumChunk;
-        for (long long e = e0 + tid; e < e0 + kSumChunk && e < tk.len; e += kThreads) {
-          double acc = 0.0;
-          for (int q = 0; q < tk.nslots; ++q) acc += double(__ldcg(tk.src + e + q * tk.stride));
-          tk.dst[e] = float(acc);
-        }
+        const long long e = (long long)(u % L.sum_units) * kSweepSumChunk + lane;
+        double acc = 0.0;
+        if (e < tk.len)
+          for (int q = w; q < tk.nslots; q += kThreads / 32)
+            acc += double(__ldcg(tk.src + e + (long long)q * tk.stride));
+        part[w * 32 + lane] = acc;
+        __syncthreads();
+        if (w == 0 && e < tk.len)
+          tk.dst[e] = float(((part[lane] + part[32 + lane]) + part[64 + lane]) + part[96 + lane]);
+        __syncthreads();
       }
     }
-    if (!grid_sync(bar, target, limit)) return;
+    if (!grid_sync(bar, gen, limit)) return;
     // node apply [eta0; eta1] = M [W0; W1]
     {
       float *Bs = reinterpret_cast<float *>(smem);
@@ -121,7 +141,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       for (int u = blockIdx.x; u < nu; u += gridDim.x)
         nn_rows_unit<NC, true>(L.ap_items, L.ap_segs, 1.f, 0.f, u / L.ap_rb, u % L.ap_rb, Bs);
     }
-    if (!grid_sync(bar, target, limit)) return;
+    if (!grid_sync(bar, gen, limit)) return;
     // broadcast d_c -= u_c eta_c
     {
       float *Bs = reinterpret_cast<float *>(smem);
@@ -129,7 +149,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       for (int u = blockIdx.x; u < nu; u += gridDim.x)
         nn_rows_unit<NC, true>(L.bc_items, L.bc_segs, -1.f, 1.f, u / L.bc_rb, u % L.bc_rb, Bs);
     }
-    if (l + 1 < nlevels && !grid_sync(bar, target, limit)) return;
+    if (l + 1 < nlevels && !grid_sync(bar, gen, limit)) return;
   }
 }
 
@@ -162,7 +182,7 @@ void launch_nc(const SweepLevel *levels, int nlevels, unsigned *bar, cudaStream_
       grid = f->second;
     }
   }
-  HODLR_CUDA_TRY(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s));
+  HODLR_CUDA_TRY(cudaMemsetAsync(bar, 0, kSweepBarWords * sizeof(unsigned), s));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(kThreads);

@@ -17,18 +17,24 @@ struct SweepLevel {
   const GemmItem<float, float> *bc_items;
   const GemmSeg<float> *bc_segs;
   int n_red, red_mt, red_nt;  // items, 64-row and 16-column blocks per item
-  int n_sums, sum_units;      // tasks, 512-element chunks per task
+  int n_sums, sum_units;      // tasks, kSweepSumChunk-element chunks per task
   int n_ap, ap_rb;            // items, 128-row blocks per item
   int n_bc, bc_rb;
 };
+
+// Slot-sum elements per work unit of the persistent kernel.
+constexpr int kSweepSumChunk = 32;
+// Words of the grid barrier: arrival counter, release word and abort flag,
+// each on its own 128-byte line.
+constexpr int kSweepBarWords = 96;
 
 // True unless the environment sets HODLR_PERSISTENT_SWEEP=0 (one launch per
 // step instead).
 bool sweep_persistent_enabled();
 
 // All levels in one cooperative launch; max_n bounds the apply / broadcast
-// items' column count (<= 32); bar: two unsigned words of device memory (the
-// grid barrier, cleared by the launch).
+// items' column count (<= 32); bar: kSweepBarWords unsigned words of device
+// memory (the grid barrier, cleared by the launch).
 void launch_sweep_levels(const SweepLevel *levels, int nlevels, int max_n, unsigned *bar,
                          cudaStream_t s);
 

@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "gemm_simt.cuh"
@@ -73,7 +74,9 @@ __device__ inline void mbar_init(uint64_t *bar, uint32_t count) {
 }
 
 // Bounded wait for the completion of phase `parity`; false on timeout.
-__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit) {
+// `suspend` is the try_wait suspend-time hint in ns (0: poll).
+__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit,
+                                 uint32_t suspend = kSuspendNs) {
   const uint32_t a = smem_u32(bar);
   for (long long it = 0; it < limit; ++it) {
     uint32_t ok;
@@ -82,7 +85,7 @@ __device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(ok)
-        : "r"(a), "r"(parity), "r"(kSuspendNs)
+        : "r"(a), "r"(parity), "r"(suspend)
         : "memory");
     if (ok) return true;
   }
@@ -219,7 +222,10 @@ constexpr int kMmaWarp = kProdWarps;
 constexpr int kEpiWarp0 = kProdWarps + 1;
 constexpr int kWarps = kProdWarps + 1 + kEpiWarps;
 constexpr int kThreadsP = kWarps * 32;
-constexpr int kStagesP = kTF32 ? 3 : 2;  // UMMA operand ring
+// UMMA operand ring: three stages where the shared memory allows it (BN = 64
+// tiles, the reduce's swapped ones among them), else two
+template <int BN>
+__host__ __device__ constexpr int stages_p() { return (kTF32 || BN == 64) ? 3 : 2; }
 constexpr int kStg = kTF32 ? 4 : 3;      // FP32 staging ring (stages in flight per producer)
 
 __device__ inline void cpa4(void *dst, const void *src, bool ok) {
@@ -316,7 +322,7 @@ template <int BN, bool SWAP, typename TC>
 __global__ void __launch_bounds__(kThreadsP, 1)
     tc_gemm_persistent(const GemmItem<float, TC> *__restrict__ items,
                        const GemmSeg<float> *__restrict__ segs, int nitems, int mtiles,
-                       int ntn, float alpha, float beta, int trans) {
+                       int ntn, float alpha, float beta, int trans, unsigned suspend) {
   static_assert(sizeof(TC) == 4, "the engine writes FP32 results");
   constexpr bool swap = SWAP;
   constexpr int A_BYTES = BM * BK * ELEM;  // one of hi / lo
@@ -326,6 +332,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
   constexpr int TMEM_COLS = 2 * BN;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char *ring = smem;
+  constexpr int kStagesP = stages_p<BN>();
   float *stg = reinterpret_cast<float *>(smem + kStagesP * STAGE_BYTES);
   float *cst = stg + kStg * (STG_BYTES / 4);  // C tile staging, 128 x (BN + 4)
   __shared__ __align__(8) uint64_t full[kStagesP], empty[kStagesP], tfull[2], tready[2], fin;
@@ -491,7 +498,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
         }
       }
       cslot = (cslot + 1) % kStg;
-      if (!mbar_wait(&empty[stage], phase ^ 1, spin_limit)) {
+      if (!mbar_wait(&empty[stage], phase ^ 1, spin_limit, suspend)) {
         abort_sh = 1;
         if (!colmode) break;
         continue;  // the group leaves together at the next vote
@@ -526,13 +533,13 @@ __global__ void __launch_bounds__(kThreadsP, 1)
         if (!decode(t, it, m0, n0, Mu, Nu)) continue;
         // the epilogue has drained this accumulator and preloaded it with
         // (beta / alpha) Cin when the item has one
-        if (!mbar_wait(&tready[acc], aphase, spin_limit)) { abort_sh = 1; break; }
+        if (!mbar_wait(&tready[acc], aphase, spin_limit, suspend)) { abort_sh = 1; break; }
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(acc * BN);
         const int nst = kstages(it);
         const uint32_t pre = (it.Cin != nullptr && beta != 0.f) ? 1u : 0u;
         for (int ks_all = 0; ks_all < nst; ++ks_all) {
-          if (!mbar_wait(&full[stage], phase, spin_limit)) { abort_sh = 1; break; }
+          if (!mbar_wait(&full[stage], phase, spin_limit, suspend)) { abort_sh = 1; break; }
           tc_fence_after();
           const uint32_t a_hi = smem_u32(ring + stage * STAGE_BYTES), a_lo = a_hi + A_BYTES;
           const uint32_t b_hi = a_hi + 2 * A_BYTES, b_lo = b_hi + B_BYTES;
@@ -554,7 +561,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
         if (++acc == 2) { acc = 0; aphase ^= 1; }
       }
       mma_commit(&fin);  // all MMAs of this CTA complete before TMEM is freed
-      if (!mbar_wait(&fin, 0, spin_limit)) abort_sh = 1;
+      if (!mbar_wait(&fin, 0, spin_limit, suspend)) abort_sh = 1;
     }
   } else {
     // ------------------------------------------------------------ epilogue
@@ -711,7 +718,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
       const GemmItem<float, TC> &it = cur.it;
       const int m0 = cur.m0, n0 = cur.n0, Mu = cur.Mu, Nu = cur.Nu;
       const bool live = kstages(it) > 0 || (it.Cin != nullptr && beta != 0.f);
-      const bool ok = mbar_wait(&tfull[acc], aphase, spin_limit);
+      const bool ok = mbar_wait(&tfull[acc], aphase, spin_limit, suspend);
       cpa_wait<0>();  // tile j + 2's Cin staged by this thread
       // one barrier: every thread's copies visible, one exit decision for all
       if (epi_vote_or(!ok || abort_sh)) {
@@ -782,11 +789,22 @@ __global__ void __launch_bounds__(kThreadsP, 1)
                  "r"(TMEM_COLS));
 }
 
+// try_wait suspend-time hint of the engine's mbarrier waits (ns), from
+// HODLR_TC_SUSPEND_NS (default kSuspendNs)
+unsigned tc_suspend_ns() {
+  static const unsigned v = [] {
+    const char *e = std::getenv("HODLR_TC_SUSPEND_NS");
+    return e ? (unsigned)std::atoi(e) : kSuspendNs;
+  }();
+  return v;
+}
+
 template <int BN, bool SWAP, typename TC>
 void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int nitems,
                int mu_max, int nu_max, bool trans, float alpha, float beta, cudaStream_t s) {
   constexpr int STAGE_BYTES = 2 * BM * BK * ELEM + 2 * BN * BK * ELEM;
   constexpr int STG_BYTES = 2 * 128 * BK * 4;
+  constexpr int kStagesP = stages_p<BN>();
   const size_t smem = (size_t)kStagesP * STAGE_BYTES + (size_t)kStg * STG_BYTES +
                       (size_t)(BN + 4) * 128 * 4 + 128;
   raise_smem_limit(reinterpret_cast<const void *>(tc_gemm_persistent<BN, SWAP, TC>), smem);
@@ -800,8 +818,8 @@ void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int
     cudaGetLastError();
   }
   const int grid = (int)std::min<long long>(total, sms);
-  tc_gemm_persistent<BN, SWAP, TC><<<grid, kThreadsP, smem, s>>>(items, segs, nitems, mt, nt,
-                                                                 alpha, beta, trans ? 1 : 0);
+  tc_gemm_persistent<BN, SWAP, TC><<<grid, kThreadsP, smem, s>>>(
+      items, segs, nitems, mt, nt, alpha, beta, trans ? 1 : 0, tc_suspend_ns());
   HODLR_LAUNCH_CHECK();
 }
 

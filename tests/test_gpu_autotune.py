@@ -49,6 +49,19 @@ def test_fp64_two_level_leaf_matches_oracle(fs, oracle, cuda, system, ob64):
     assert relerr(h.solution(), Xo[:, :M]) < 1e-12
 
 
+def test_fp64_two_level_leaf_large_grid(fs, oracle, cuda):
+    """The block-row solves of the two-level FP64 leaf LU are in-place products
+    (C = L^{-1} C): with 256 leaves their launches hold thousands of tiles,
+    and a tiling that split one item's 128 rows over two CTAs would let one
+    CTA overwrite rows the other still reads."""
+    s = oracle.gaussian_system(131072, 4, 32, 512, seed=41)
+    h = _load(fs, s, 131072, 4, 32, 512)
+    h.schedule = dict(leaf_ob64=128)
+    fs.FastSolver().bfs_solve(h)
+    Xo, _ = oracle.bfs_solve(s, nthreads=8)
+    assert relerr(h.solution(), Xo[:, :4]) < 1e-12
+
+
 def test_fp64_two_level_leaf_1024_rows(fs, oracle, cuda):
     """Leaves above 512 rows take 16-wide FP64 panels: 8 of them per block."""
     s = oracle.gaussian_system(9001, 3, 40, 1024, seed=5)
