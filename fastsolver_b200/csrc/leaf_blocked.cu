@@ -269,7 +269,7 @@ __device__ inline void warp_argmax(double &best, int &pos, int &code, int &wlane
   if (!win) code = -1;
 }
 
-template <typename T, int NB, int RPT, int QWR>
+template <typename T, int NB, int RPT>
 __global__ void __launch_bounds__(kRegThreads, 1)
     leaf_panel_reg_kernel(const LeafFactorTask<T> *__restrict__ tasks, int k0, int panel,
                           int *info) {
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kRegThreads, 1)
   // rotated left by h QW, so the quarter's columns sit at register positions
   // 0 .. QW - 1; positions QW .. NB - h QW - 1 hold the later quarters (they
   // are updated), the rest the finished ones (left alone).
-  constexpr int QW = NB < QWR ? NB : QWR;
+  constexpr int QW = NB < 16 ? NB : 16;
   constexpr int NQ = NB / QW;
 #pragma unroll 1
   for (int h = 0; h < NQ; ++h) {
@@ -899,27 +899,12 @@ void launch_leaf_panel_nb(const LeafFactorTask<T> *tasks, int count, int max_n, 
   HODLR_LAUNCH_CHECK();
 }
 
-// Columns per unrolled body of the register panel (HODLR_PANEL_QW: 16, 8 or
-// 4; default 16): a smaller body is less code for the instruction cache and
-// one more row rotation per QW columns.
-int panel_qw() {
-  static const int qw = [] {
-    const char *e = std::getenv("HODLR_PANEL_QW");
-    const int v = e ? std::atoi(e) : 16;
-    return (v == 4 || v == 8) ? v : 16;
-  }();
-  return qw;
-}
-
 template <typename T, int NB, int RPT>
 void launch_leaf_panel_reg(const LeafFactorTask<T> *tasks, int count, int rows, int k0,
                            int panel, int *info, cudaStream_t s) {
   // one warp per 32 x RPT live rows of the largest leaf's panel
   const int threads = std::min(kRegThreads, std::max(32, cdiv(cdiv(rows, RPT), 32) * 32));
-  const int qw = panel_qw();
-  if (qw == 4) leaf_panel_reg_kernel<T, NB, RPT, 4><<<count, threads, 0, s>>>(tasks, k0, panel, info);
-  else if (qw == 8) leaf_panel_reg_kernel<T, NB, RPT, 8><<<count, threads, 0, s>>>(tasks, k0, panel, info);
-  else leaf_panel_reg_kernel<T, NB, RPT, 16><<<count, threads, 0, s>>>(tasks, k0, panel, info);
+  leaf_panel_reg_kernel<T, NB, RPT><<<count, threads, 0, s>>>(tasks, k0, panel, info);
   HODLR_LAUNCH_CHECK();
 }
 

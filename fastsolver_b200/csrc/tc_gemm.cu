@@ -789,16 +789,6 @@ __global__ void __launch_bounds__(kThreadsP, 1)
                  "r"(TMEM_COLS));
 }
 
-// try_wait suspend-time hint of the engine's mbarrier waits (ns), from
-// HODLR_TC_SUSPEND_NS (default kSuspendNs)
-unsigned tc_suspend_ns() {
-  static const unsigned v = [] {
-    const char *e = std::getenv("HODLR_TC_SUSPEND_NS");
-    return e ? (unsigned)std::atoi(e) : kSuspendNs;
-  }();
-  return v;
-}
-
 template <int BN, bool SWAP, typename TC>
 void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int nitems,
                int mu_max, int nu_max, bool trans, float alpha, float beta, cudaStream_t s) {
@@ -819,7 +809,7 @@ void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int
   }
   const int grid = (int)std::min<long long>(total, sms);
   tc_gemm_persistent<BN, SWAP, TC><<<grid, kThreadsP, smem, s>>>(
-      items, segs, nitems, mt, nt, alpha, beta, trans ? 1 : 0, tc_suspend_ns());
+      items, segs, nitems, mt, nt, alpha, beta, trans ? 1 : 0, kSuspendNs);
   HODLR_LAUNCH_CHECK();
 }
 
