@@ -7,20 +7,21 @@
 // as  A_hi B_hi + A_hi B_lo + A_lo B_hi  (the lo*lo term, ~2^-16 relative, is
 // dropped; FP64 iterative refinement recovers full accuracy).
 //
-// One CTA (128 threads) computes a 128 x BN tile of one item:
-//   * every thread owns one row of the A tile and one (or two) rows of the B
-//     tile, loads its 32 K-values per stage from global memory (coalesced
-//     across threads for the M-contiguous operands, 128-byte rows for the
-//     K-contiguous ones), keeps the next stage's values in registers while the
-//     current one is converted, and writes hi/lo bf16 into the UMMA canonical
-//     K-major layout (8-row x 16-byte core matrices, no swizzle);
-//   * a 3-stage shared-memory ring; thread 0 issues the MMAs
-//     (tcgen05.mma.cta_group::1.kind::f16, M = 128, N = BN, K = 16) and
+// One persistent CTA per SM (17 warps) computes 128 x BN tiles of the items:
+//   * two 4-warp producer groups (A tile, B tile) stage 32 K-values per row
+//     and stage from global memory with cp.async, a few stages ahead, each
+//     group cooperatively (whole 128-byte row runs or 512-byte column runs
+//     per warp instruction); then every producer thread splits its own row
+//     into hi/lo bf16 in the UMMA canonical K-major layout (8-row x 16-byte
+//     core matrices, no swizzle);
+//   * a 2- or 3-stage UMMA operand ring; one lane of the MMA warp issues the
+//     MMAs (tcgen05.mma.cta_group::1.kind::f16, M = 128, N = BN, K = 16) and
 //     tcgen05.commit arrives on the stage's mbarrier when the tensor cores are
 //     done with it; producers wait on that barrier before reusing the stage;
-//   * the accumulator lives in TMEM (BN columns, allocated per CTA); the
-//     epilogue reads it with tcgen05.ld (32 lanes per warp) and writes
-//     alpha * acc + beta * Cin to global memory.
+//   * two accumulators live in TMEM (BN columns each, allocated per CTA); the
+//     epilogue warps read one with tcgen05.ld (32 lanes per warp) and write
+//     alpha * acc + beta * Cin to global memory while the next tile
+//     accumulates into the other.
 // The reduce's V^T X (M = r small, N wide) runs "swapped": the UMMA M side is
 // the item's N and the result is written transposed.
 // Every mbarrier wait is bounded; on timeout the kernel raises g_tc_error,
@@ -47,17 +48,15 @@ __device__ int g_tc_skip_commit = 0;
 namespace {
 
 constexpr int BM = 128;    // UMMA M
-// Operand split.  BF16 (kind::f16, the default): hi = bf16(x), lo = bf16(x - hi),
-// each product accurate to ~2^-16 relative.  TF32 (kind::tf32, compile-time
-// alternative): hi = tf32(x), lo = tf32(x - hi), ~2^-21.  Both keep 64 bytes
-// of K per operand row and stage (two MMA k-steps), so the canonical smem
-// layout is the same.  Measured at N = 262144 (r = 64, m = 16): both need
-// two FP64 refinement sweeps to reach 1e-12 (after one sweep 2.8e-11 with
-// TF32, 9.6e-13 with plain FP32 FMA), so the cheaper BF16 split is used.
-constexpr bool kTF32 = false;
-constexpr int ELEM = kTF32 ? 4 : 2;  // bytes per split operand element
-constexpr int BK = 64 / ELEM;        // K per stage
-constexpr int MMA_K = 32 / ELEM;     // K per tcgen05.mma
+// Operand split: hi = bf16(x), lo = bf16(x - hi) (kind::f16), each product
+// accurate to ~2^-16 relative.  A TF32 split (kind::tf32, ~2^-21) was
+// measured at N = 262144 (r = 64, m = 16): both need two FP64 refinement
+// sweeps to reach 1e-12 (after one sweep 2.8e-11 with TF32, 9.6e-13 with
+// plain FP32 FMA), so the cheaper BF16 split is used; its hi / lo pair also
+// takes exactly the bytes of the FP32 value, so a stage is split in place.
+constexpr int ELEM = 2;    // bytes per split operand element
+constexpr int BK = 32;     // K per stage: 64 bytes of hi (and of lo) per operand row
+constexpr int MMA_K = 16;  // K per tcgen05.mma kind::f16
 // Bounded mbarrier waits: each try_wait may suspend the thread for up to
 // kSuspendNs (it returns as soon as the phase completes), so waiting warps
 // do not take issue slots from the working ones; g_tc_spin_limit tries
@@ -113,12 +112,11 @@ __device__ inline uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t
   return d;
 }
 
-// Instruction descriptor: kind::tf32 (A = B = TF32) or kind::f16 (A = B =
-// BF16), D = F32, both K-major.
+// Instruction descriptor: kind::f16 with A = B = BF16, D = F32, both K-major.
 __host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
   return (1u << 4)                       // D format F32
-         | ((kTF32 ? 2u : 1u) << 7)      // A format
-         | ((kTF32 ? 2u : 1u) << 10)     // B format
+         | (1u << 7)                     // A format BF16
+         | (1u << 10)                    // B format BF16
          | ((uint32_t)(N >> 3) << 17)    // N
          | ((uint32_t)(M >> 4) << 24);   // M
 }
@@ -126,21 +124,12 @@ __host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
 __device__ inline void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
                                 uint32_t accumulate) {
   const uint32_t z = 0;  // disable-output-lane mask: all lanes written
-  if constexpr (kTF32) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-            tmem_d),
-        "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
-  } else {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-            tmem_d),
-        "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
-  }
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+          tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
 __device__ inline void mma_commit(uint64_t *bar) {
@@ -174,38 +163,16 @@ __device__ inline void split_store8(const float *v, unsigned char *hi, unsigned 
   *reinterpret_cast<uint4 *>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// Split 4 FP32 values into hi / lo tf32 and store one 16-byte chunk of each.
-__device__ inline void split_store4_tf32(const float *v, unsigned char *hi, unsigned char *lo,
-                                         uint32_t off) {
-  uint32_t h[4], l[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h[q]) : "f"(v[q]));
-    const float r = v[q] - __uint_as_float(h[q]);
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l[q]) : "f"(r));
-  }
-  *reinterpret_cast<uint4 *>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-  *reinterpret_cast<uint4 *>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
-}
-
-// One 16-byte chunk (16 / ELEM values) of each split operand.
-__device__ inline void split_chunk(const float *v, unsigned char *hi, unsigned char *lo,
-                                   uint32_t off) {
-  if constexpr (kTF32) split_store4_tf32(v, hi, lo, off);
-  else split_store8(v, hi, lo, off);
-}
-
 __device__ inline void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // Persistent, warp-specialized split-operand GEMM.
-//   warps 0-7 (producers): thread p of warps 0-3 owns row p of the A tile,
-//     of warps 4-7 row p of the B tile.  It stages its rows' FP32 values with asynchronous cp.async
-//     copies kStg stages ahead into its own slot of a staging ring (so a
-//     per-thread cp.async.wait_group suffices), then splits the landed stage
-//     into hi / lo and writes the UMMA K-major ring (full[s]: 128 arrivals,
-//     empty[s]: tcgen05.commit).
+//   warps 0-7 (producers): warps 0-3 stage the A tile, warps 4-7 the B tile,
+//     each group cooperatively with cp.async, ring_depth<BN>() - 1 stages
+//     ahead (cp.async.wait_group, then the group's named barrier); thread p
+//     then splits row p of its tile into hi / lo in place, in the UMMA
+//     K-major layout (full[s]: 256 arrivals, empty[s]: tcgen05.commit).
 //   warp 8 lane 0 (MMA issuer): 3 MMAs per k-step into one of two TMEM
 //     accumulators (tfull[a]: commit; tready[a]: one arrival per epilogue
 //     thread once the buffer is drained and preloaded with the next tile's
@@ -222,11 +189,26 @@ constexpr int kMmaWarp = kProdWarps;
 constexpr int kEpiWarp0 = kProdWarps + 1;
 constexpr int kWarps = kProdWarps + 1 + kEpiWarps;
 constexpr int kThreadsP = kWarps * 32;
-// UMMA operand ring: three stages where the shared memory allows it (BN = 64
-// tiles, the reduce's swapped ones among them), else two
+// One ring of stages, each the A tile (128 rows) and the B tile (BN rows) of
+// BK k-values: the cp.async copies land there as FP32, and each producer
+// thread then overwrites its row with the hi / lo bf16 split in the UMMA
+// canonical layout (the same bytes), which the MMAs read.  Measured on this
+// part: scattered 128-byte row runs read at 2.3 TB/s with 64 KB per SM in
+// flight, 4.1 TB/s with 128 KB and 4.6 TB/s with 256 KB (a stage lands 3-5 us
+// after its copies are issued under load), so the ring is as deep as the
+// shared memory allows next to the C staging: 5 stages of 32 KB for
+// 128-column tiles, 8 of 24 KB for 64-column ones.
 template <int BN>
-__host__ __device__ constexpr int stages_p() { return (kTF32 || BN == 64) ? 3 : 2; }
-constexpr int kStg = kTF32 ? 4 : 3;      // FP32 staging ring (stages in flight per producer)
+__host__ __device__ constexpr int stage_bytes() { return (128 + BN) * BK * 4; }
+template <int BN>
+__host__ __device__ constexpr int cst_bytes() { return (BN + 4) * 128 * 4; }
+constexpr int kSmemPerCta = 232448;  // 227 KB opt-in shared memory per CTA
+constexpr int kStaticSmem = 256;     // the kernel's barriers and flags
+constexpr int kRefillLag = 2;
+template <int BN>
+__host__ __device__ constexpr int ring_depth() {
+  return (kSmemPerCta - kStaticSmem - 128 - cst_bytes<BN>()) / stage_bytes<BN>();
+}
 
 __device__ inline void cpa4(void *dst, const void *src, bool ok) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
@@ -251,43 +233,30 @@ struct KPos {
   bool valid;
 };
 
-// Stage one row's BK values of an operand into `dst` (BK floats, the
-// thread's own staging row) with cp.async; zero-filled outside the matrix.
-// The row's eight 16-byte chunks are XOR-swizzled by `sw` (= row & 7) so that
-// the 32 lanes reading their rows chunk by chunk hit distinct banks.
+// Stage one row of an M-contiguous operand (row `row`, its BK k-values ld
+// apart) into `dst` (BK floats, the thread's own staging row) with 4-byte
+// cp.async copies; consecutive lanes own consecutive rows, so each warp
+// instruction reads 128 contiguous bytes.  Zero-filled outside the matrix.
+// The row's 16-byte chunks are XOR-swizzled by `sw` (= row & 7) so that the
+// 32 lanes reading their rows chunk by chunk hit distinct banks.
 __device__ inline void cpa4_u(void *dst, const void *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(dst)), "l"(src));
 }
-__device__ inline void stage_row(float *dst, int sw, const float *base, long long ld,
-                                 bool kcontig, int row, int rows_valid, int k0, int K) {
+__device__ inline void stage_row_strided(float *dst, int sw, const float *base, long long ld,
+                                         int row, int rows_valid, int k0, int K) {
   float *chunk[BK / 4];
 #pragma unroll
   for (int g = 0; g < BK / 4; ++g) chunk[g] = dst + ((g ^ sw) << 2);
   const bool inrow = row < rows_valid;
-  const bool full = inrow && k0 + BK <= K;
-  if (kcontig) {
-    const float *p = base + (long long)row * ld + k0;
-    if (full && ((reinterpret_cast<uintptr_t>(p) & 15) == 0)) {
+  const float *p = base + row + (long long)k0 * ld;
+  if (inrow && k0 + BK <= K) {
 #pragma unroll
-      for (int g = 0; g < BK / 4; ++g) cpa16(chunk[g], p + 4 * g);
-    } else {
-#pragma unroll
-      for (int k = 0; k < BK; ++k) {
-        const bool ok = inrow && k0 + k < K;
-        cpa4(chunk[k >> 2] + (k & 3), ok ? p + k : base, ok);
-      }
-    }
+    for (int k = 0; k < BK; ++k) cpa4_u(chunk[k >> 2] + (k & 3), p + (long long)k * ld);
   } else {
-    const float *p = base + row + (long long)k0 * ld;
-    if (full) {
 #pragma unroll
-      for (int k = 0; k < BK; ++k) cpa4_u(chunk[k >> 2] + (k & 3), p + (long long)k * ld);
-    } else {
-#pragma unroll
-      for (int k = 0; k < BK; ++k) {
-        const bool ok = inrow && k0 + k < K;
-        cpa4(chunk[k >> 2] + (k & 3), ok ? p + (long long)k * ld : base, ok);
-      }
+    for (int k = 0; k < BK; ++k) {
+      const bool ok = inrow && k0 + k < K;
+      cpa4(chunk[k >> 2] + (k & 3), ok ? p + (long long)k * ld : base, ok);
     }
   }
 }
@@ -318,6 +287,43 @@ __device__ inline void stage_cols(float *dst, int wg, int lane, const float *bas
   }
 }
 
+// Stage NROWS K-contiguous operand rows (row r: base[(row0 + r) ld + k0 ..
+// + BK)) into the group's staging region, cooperatively: thread t of the
+// 4-warp group copies 16-byte chunk t % CPR of rows t / CPR, t / CPR +
+// 128 / CPR, ... (CPR = BK / 4 chunks per row), so that one BF16-split warp
+// instruction covers four whole 128-byte row runs (one L2 request each)
+// instead of a 16-byte piece of 32 different rows.  Row r lands at dst + r BK
+// with its chunks XOR-swizzled like stage_row_strided's, the layout that thread r
+// reads back.  Zero-filled outside the matrix.
+template <int NROWS>
+__device__ inline void stage_rows_coop(float *dst, int t, const float *base, long long ld,
+                                       int row0, int rows_valid, int k0, int K) {
+  constexpr int CPR = BK / 4;
+  constexpr int RPP = 128 / CPR;  // rows per pass of the group
+  static_assert(NROWS % RPP == 0, "whole passes");
+  const int c = t % CPR;
+  const int kc = k0 + 4 * c;
+  const bool vec = ((reinterpret_cast<uintptr_t>(base) & 15) == 0) && ((ld & 3) == 0);
+  const bool kfull = kc + 4 <= K;
+#pragma unroll
+  for (int i = 0; i < NROWS / RPP; ++i) {
+    const int r = t / CPR + RPP * i;
+    const int gr = row0 + r;
+    const int sw = r & 7;
+    float *d = dst + r * BK + ((c ^ sw) << 2);
+    const float *src = base + (long long)gr * ld + kc;
+    if (vec && kfull && gr < rows_valid) {
+      cpa16(d, src);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool ok = gr < rows_valid && kc + u < K;
+        cpa4(d + u, ok ? src + u : base, ok);
+      }
+    }
+  }
+}
+
 template <int BN, bool SWAP, typename TC>
 __global__ void __launch_bounds__(kThreadsP, 1)
     tc_gemm_persistent(const GemmItem<float, TC> *__restrict__ items,
@@ -328,13 +334,13 @@ __global__ void __launch_bounds__(kThreadsP, 1)
   constexpr int A_BYTES = BM * BK * ELEM;  // one of hi / lo
   constexpr int B_BYTES = BN * BK * ELEM;
   constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-  constexpr int STG_BYTES = 2 * 128 * BK * 4;  // A and B rows of the 128 producers
+  static_assert(STAGE_BYTES == stage_bytes<BN>(), "the split fills the FP32 stage exactly");
+  constexpr int kStagesP = ring_depth<BN>();
+  static_assert(kStagesP >= 3, "at least one stage in flight while one is split");
   constexpr int TMEM_COLS = 2 * BN;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char *ring = smem;
-  constexpr int kStagesP = stages_p<BN>();
-  float *stg = reinterpret_cast<float *>(smem + kStagesP * STAGE_BYTES);
-  float *cst = stg + kStg * (STG_BYTES / 4);  // C tile staging, 128 x (BN + 4)
+  float *cst = reinterpret_cast<float *>(smem + kStagesP * STAGE_BYTES);  // C tile, 128 x (BN + 4)
   __shared__ __align__(8) uint64_t full[kStagesP], empty[kStagesP], tfull[2], tready[2], fin;
   __shared__ uint32_t tmem_sh;
   __shared__ volatile int abort_sh;
@@ -420,45 +426,50 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     // B tile (rows p >= BN of B do not exist)
     const bool isB = warp >= 4;
     const int p = tid & 127;
-    const int sw = kTF32 ? ((p >> 1) & 3) : (p & 7);
+    const int sw = p & 7;
     KPos<TC> iss, con;
     iss.t = con.t = blockIdx.x;
     first_in_tile(iss);
     first_in_tile(con);
-    // the non-K-contiguous operand (A when !trans) is staged column-wise by
-    // its whole 4-warp group; the other one row-wise by each thread
-    // (measured: worth it for the non-swapped A tile only; the swapped items'
-    // non-contiguous operand has BN <= 64 rows and stays row-wise)
+    // Each 4-warp group stages its operand cooperatively and synchronizes on
+    // its own named barrier before reading a landed stage and before
+    // overwriting it with the split: the M-contiguous A tile (A when !trans)
+    // column-wise (stage_cols), K-contiguous rows 8 lanes per 128-byte run
+    // (stage_rows_coop).  Only the swapped items' M-contiguous operand (at
+    // most BN = 64 rows, one 4-byte column element per thread and k, i.e.
+    // 128 contiguous bytes per warp instruction) is staged by each row's
+    // owner.
     const bool colmode = !isB && !swap && trans == 0;
     const int gbar = isB ? 3 : 2;  // named barrier of this producer group
     auto group_sync = [&]() { asm volatile("bar.sync %0, 128;\n" ::"r"(gbar) : "memory"); };
+    // this group's part of ring slot `slot`: FP32 rows as staged, then the
+    // same bytes as hi | lo (A: 128 rows at the slot's start; B: BN rows
+    // after them)
+    auto part_of = [&](int slot) { return ring + slot * STAGE_BYTES + (isB ? 2 * A_BYTES : 0); };
     auto issue = [&](KPos<TC> &ps, int slot) {
-      float *region = stg + slot * (STG_BYTES / 4) + (isB ? 128 * BK : 0);
-      float *row = region + p * BK;
+      float *region = reinterpret_cast<float *>(part_of(slot));
       if (ps.valid) {
         const GemmSeg<float> &sg = ps.sg;
         if (!isB) {
           if (!swap) {
             if (colmode) stage_cols(region, warp & 3, lane, sg.A, sg.lda, ps.m0, ps.it.M, ps.k0, sg.K);
-            else stage_row(row, sw, sg.A, sg.lda, trans != 0, ps.m0 + p, ps.it.M, ps.k0, sg.K);
+            else stage_rows_coop<128>(region, p, sg.A, sg.lda, ps.m0, ps.it.M, ps.k0, sg.K);
           } else {
-            stage_row(row, sw, sg.B, sg.ldb, true, ps.m0 + p, ps.it.N, ps.k0, sg.K);
+            stage_rows_coop<128>(region, p, sg.B, sg.ldb, ps.m0, ps.it.N, ps.k0, sg.K);
           }
         } else {
           if (!swap) {
-            if (p < BN) stage_row(row, sw, sg.B, sg.ldb, true, ps.n0 + p, ps.it.N, ps.k0, sg.K);
+            stage_rows_coop<BN>(region, p, sg.B, sg.ldb, ps.n0, ps.it.N, ps.k0, sg.K);
+          } else if (trans != 0) {
+            stage_rows_coop<BN>(region, p, sg.A, sg.lda, ps.n0, ps.it.M, ps.k0, sg.K);
           } else if (p < BN) {
-            stage_row(row, sw, sg.A, sg.lda, trans != 0, ps.n0 + p, ps.it.M, ps.k0, sg.K);
+            stage_row_strided(region + p * BK, sw, sg.A, sg.lda, ps.n0 + p, ps.it.M, ps.k0, sg.K);
           }
         }
         next(ps);
       }
       cpa_commit();
     };
-    int islot = 0;
-    for (int i = 0; i < kStg - 1; ++i) { issue(iss, islot); islot = (islot + 1) % kStg; }
-    int stage = 0, cslot = 0;
-    uint32_t phase = 0;
     // exit decision: uniform within a group that shares barriers (a thread
     // whose wait timed out raises abort_sh and the next vote ends the group)
     auto group_vote_or = [&](bool pr) -> bool {
@@ -473,49 +484,57 @@ __global__ void __launch_bounds__(kThreadsP, 1)
           : "memory");
       return r != 0;
     };
-    while (true) {
-      if (colmode) {
-        if (group_vote_or(!con.valid || abort_sh)) break;
-      } else if (!con.valid || abort_sh) {
-        break;
-      }
-      issue(iss, islot);
-      islot = (islot + 1) % kStg;
-      cpa_wait<kStg - 1>();  // this thread's copies of stage `cslot` have landed
-      const float *region = stg + cslot * (STG_BYTES / 4) + (isB ? 128 * BK : 0);
+    // Stage s lives in slot s % D.  Stages 0 .. D - L - 1 are issued up
+    // front; iteration s waits for stage s, splits it in place, hands it to
+    // the MMA warp (full), then refills slot (s - L) % D -- freed by the MMAs
+    // of stage s - L (empty) -- with stage s + D - L, so D - L - 1 stages stay
+    // in flight while one is split.  The lag L covers the MMAs' completion
+    // latency.  con advances alike in every thread (timeouts included), so
+    // the loop condition is uniform across the group.
+    constexpr int D = kStagesP;
+    constexpr int L = kRefillLag;
+    static_assert(D - L - 1 >= 1, "a stage in flight while one is split");
+    for (int i = 0; i < D - L; ++i) issue(iss, i);
+    int slot = 0;           // slot of stage s
+    int rslot = D - L;      // slot refilled in iteration s: the one of stage s - L
+    uint32_t rphase = 1;    // parity of the empty phase that frees it (fresh: 1)
+    while (con.valid) {
+      cpa_wait<D - L - 1>();  // this thread's copies of stage s have landed
+      group_sync();       // ... and the whole group's
+      unsigned char *part = part_of(slot);
       float v[BK];
       if (colmode) {
-        group_sync();  // the group's copies of this stage have landed
+        const float *col = reinterpret_cast<const float *>(part);
 #pragma unroll
-        for (int k = 0; k < BK; ++k) v[k] = region[k * 128 + p];
-        group_sync();  // every thread has read the slot before it is refilled
+        for (int k = 0; k < BK; ++k) v[k] = col[k * 128 + p];
       } else {
-        const float *row = region + p * BK;
+        const float *row = reinterpret_cast<const float *>(part) + p * BK;
 #pragma unroll
         for (int q = 0; q < BK / 4; ++q) {
           const float4 x = reinterpret_cast<const float4 *>(row)[q ^ sw];
           v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
         }
       }
-      cslot = (cslot + 1) % kStg;
-      if (!mbar_wait(&empty[stage], phase ^ 1, spin_limit, suspend)) {
-        abort_sh = 1;
-        if (!colmode) break;
-        continue;  // the group leaves together at the next vote
-      }
-      unsigned char *base = ring + stage * STAGE_BYTES;
+      // every thread has read its FP32 row before the part is overwritten;
+      // the same barrier makes the group's exit decision
+      if (group_vote_or(abort_sh)) break;
       if (!isB) {
-        unsigned char *ahi = base, *alo = base + A_BYTES;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) split_chunk(v + (16 / ELEM) * c, ahi, alo, kmajor_off(BM, p, c));
+        for (int c = 0; c < 4; ++c) split_store8(v + 8 * c, part, part + A_BYTES, kmajor_off(BM, p, c));
       } else if (p < BN) {
-        unsigned char *bhi = base + 2 * A_BYTES, *blo = bhi + B_BYTES;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) split_chunk(v + (16 / ELEM) * c, bhi, blo, kmajor_off(BN, p, c));
+        for (int c = 0; c < 4; ++c) split_store8(v + 8 * c, part, part + B_BYTES, kmajor_off(BN, p, c));
       }
       fence_proxy_async();
-      mbar_arrive(&full[stage]);
-      if (++stage == kStagesP) { stage = 0; phase ^= 1; }
+      mbar_arrive(&full[slot]);
+      if (mbar_wait(&empty[rslot], rphase, spin_limit, suspend)) {
+        issue(iss, rslot);
+      } else {
+        abort_sh = 1;  // the group leaves together at the next vote
+        cpa_commit();  // keep one copy group per stage
+      }
+      if (++rslot == D) { rslot = 0; rphase ^= 1; }
+      if (++slot == D) slot = 0;
       next(con);
     }
     cpa_wait<0>();
@@ -792,11 +811,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
 template <int BN, bool SWAP, typename TC>
 void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int nitems,
                int mu_max, int nu_max, bool trans, float alpha, float beta, cudaStream_t s) {
-  constexpr int STAGE_BYTES = 2 * BM * BK * ELEM + 2 * BN * BK * ELEM;
-  constexpr int STG_BYTES = 2 * 128 * BK * 4;
-  constexpr int kStagesP = stages_p<BN>();
-  const size_t smem = (size_t)kStagesP * STAGE_BYTES + (size_t)kStg * STG_BYTES +
-                      (size_t)(BN + 4) * 128 * 4 + 128;
+  const size_t smem = (size_t)ring_depth<BN>() * stage_bytes<BN>() + cst_bytes<BN>() + 128;
   raise_smem_limit(reinterpret_cast<const void *>(tc_gemm_persistent<BN, SWAP, TC>), smem);
   const int mt = cdiv(mu_max, BM), nt = cdiv(nu_max, BN);
   const long long total = (long long)nitems * mt * nt;
