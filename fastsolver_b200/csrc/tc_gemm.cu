@@ -204,10 +204,20 @@ template <int BN>
 __host__ __device__ constexpr int cst_bytes() { return (BN + 4) * 128 * 4; }
 constexpr int kSmemPerCta = 232448;  // 227 KB opt-in shared memory per CTA
 constexpr int kStaticSmem = 256;     // the kernel's barriers and flags
-constexpr int kRefillLag = 2;
+// A group refills the slot of its stage i - kRefillLag after handing stage i
+// to the MMA warp (the MMAs of a stage complete ~0.2 us after their commit).
+constexpr int kRefillLag = 1;
 template <int BN>
 __host__ __device__ constexpr int ring_depth() {
   return (kSmemPerCta - kStaticSmem - 128 - cst_bytes<BN>()) / stage_bytes<BN>();
+}
+// Independent copy / split loops per CTA: on this part one loop with a deep
+// ring reads scattered 128-byte row runs at ~2.8 TB/s over the GPU whatever
+// its depth (cp.async or TMA), two loops per SM at ~3.8-4.2 TB/s.  Two where
+// the ring splits into two halves of at least 3 stages (64-column tiles).
+template <int BN>
+__host__ __device__ constexpr int prod_streams() {
+  return (ring_depth<BN>() % 2 == 0 && ring_depth<BN>() / 2 - kRefillLag - 1 >= 1) ? 2 : 1;
 }
 
 __device__ inline void cpa4(void *dst, const void *src, bool ok) {
@@ -350,7 +360,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
 
   if (tid == 0) {
     for (int s = 0; s < kStagesP; ++s) {
-      mbar_init(&full[s], kProdWarps * 32);
+      mbar_init(&full[s], kProdWarps * 32 / prod_streams<BN>());
       mbar_init(&empty[s], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -422,42 +432,60 @@ __global__ void __launch_bounds__(kThreadsP, 1)
 
   if (warp < kProdWarps) {
     // ------------------------------------------------------------ producers
-    // warps 0-3 stage and split row p of the A tile, warps 4-7 row p of the
-    // B tile (rows p >= BN of B do not exist)
-    const bool isB = warp >= 4;
+    // NS == 1: group 0 (warps 0-3) stages and splits the A tile, group 1
+    // (warps 4-7) the B tile of every stage.  NS == 2: group g stages and
+    // splits both tiles of the stages s = g (mod 2), in its own half of the
+    // ring (the slots of parity g): two independent copy / split loops per
+    // SM.  Thread p owns row p of each tile it splits (rows p >= BN of the B
+    // tile do not exist).
+    constexpr int NS = prod_streams<BN>();
+    const int grp = warp >> 2;
+    const bool doA = NS == 2 || grp == 0;
+    const bool doB = NS == 2 || grp == 1;
     const int p = tid & 127;
     const int sw = p & 7;
     KPos<TC> iss, con;
     iss.t = con.t = blockIdx.x;
     first_in_tile(iss);
     first_in_tile(con);
-    // Each 4-warp group stages its operand cooperatively and synchronizes on
-    // its own named barrier before reading a landed stage and before
-    // overwriting it with the split: the M-contiguous A tile (A when !trans)
-    // column-wise (stage_cols), K-contiguous rows 8 lanes per 128-byte run
+    auto adv = [&](KPos<TC> &ps) {
+#pragma unroll
+      for (int i = 0; i < NS; ++i)
+        if (ps.valid) next(ps);
+    };
+    if (NS == 2 && grp == 1) {  // group 1 starts at stage 1
+      if (iss.valid) next(iss);
+      if (con.valid) next(con);
+    }
+    // Each group stages cooperatively and synchronizes on its own named
+    // barrier before reading a landed stage and before overwriting it with
+    // the split: the M-contiguous A tile (A when !trans) column-wise
+    // (stage_cols), K-contiguous rows 8 lanes per 128-byte run
     // (stage_rows_coop).  Only the swapped items' M-contiguous operand (at
     // most BN = 64 rows, one 4-byte column element per thread and k, i.e.
     // 128 contiguous bytes per warp instruction) is staged by each row's
     // owner.
-    const bool colmode = !isB && !swap && trans == 0;
-    const int gbar = isB ? 3 : 2;  // named barrier of this producer group
+    const bool colmode = !swap && trans == 0;  // of the A tile
+    const int gbar = 2 + grp;                  // named barrier of this producer group
     auto group_sync = [&]() { asm volatile("bar.sync %0, 128;\n" ::"r"(gbar) : "memory"); };
-    // this group's part of ring slot `slot`: FP32 rows as staged, then the
-    // same bytes as hi | lo (A: 128 rows at the slot's start; B: BN rows
-    // after them)
-    auto part_of = [&](int slot) { return ring + slot * STAGE_BYTES + (isB ? 2 * A_BYTES : 0); };
+    // ring slot `slot`: the A tile's FP32 rows at its start, then the same
+    // bytes as A_hi | A_lo; the B tile's (BN rows) after them, then B_hi | B_lo
+    auto a_part = [&](int slot) { return ring + slot * STAGE_BYTES; };
+    auto b_part = [&](int slot) { return ring + slot * STAGE_BYTES + 2 * A_BYTES; };
     auto issue = [&](KPos<TC> &ps, int slot) {
-      float *region = reinterpret_cast<float *>(part_of(slot));
       if (ps.valid) {
         const GemmSeg<float> &sg = ps.sg;
-        if (!isB) {
+        if (doA) {
+          float *region = reinterpret_cast<float *>(a_part(slot));
           if (!swap) {
             if (colmode) stage_cols(region, warp & 3, lane, sg.A, sg.lda, ps.m0, ps.it.M, ps.k0, sg.K);
             else stage_rows_coop<128>(region, p, sg.A, sg.lda, ps.m0, ps.it.M, ps.k0, sg.K);
           } else {
             stage_rows_coop<128>(region, p, sg.B, sg.ldb, ps.m0, ps.it.N, ps.k0, sg.K);
           }
-        } else {
+        }
+        if (doB) {
+          float *region = reinterpret_cast<float *>(b_part(slot));
           if (!swap) {
             stage_rows_coop<BN>(region, p, sg.B, sg.ldb, ps.n0, ps.it.N, ps.k0, sg.K);
           } else if (trans != 0) {
@@ -466,7 +494,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
             stage_row_strided(region + p * BK, sw, sg.A, sg.lda, ps.n0 + p, ps.it.M, ps.k0, sg.K);
           }
         }
-        next(ps);
+        adv(ps);
       }
       cpa_commit();
     };
@@ -484,58 +512,78 @@ __global__ void __launch_bounds__(kThreadsP, 1)
           : "memory");
       return r != 0;
     };
-    // Stage s lives in slot s % D.  Stages 0 .. D - L - 1 are issued up
-    // front; iteration s waits for stage s, splits it in place, hands it to
-    // the MMA warp (full), then refills slot (s - L) % D -- freed by the MMAs
-    // of stage s - L (empty) -- with stage s + D - L, so D - L - 1 stages stay
-    // in flight while one is split.  The lag L covers the MMAs' completion
-    // latency.  con advances alike in every thread (timeouts included), so
-    // the loop condition is uniform across the group.
-    constexpr int D = kStagesP;
-    constexpr int L = kRefillLag;
-    static_assert(D - L - 1 >= 1, "a stage in flight while one is split");
-    for (int i = 0; i < D - L; ++i) issue(iss, i);
-    int slot = 0;           // slot of stage s
-    int rslot = D - L;      // slot refilled in iteration s: the one of stage s - L
-    uint32_t rphase = 1;    // parity of the empty phase that frees it (fresh: 1)
-    while (con.valid) {
-      cpa_wait<D - L - 1>();  // this thread's copies of stage s have landed
-      group_sync();       // ... and the whole group's
-      unsigned char *part = part_of(slot);
-      float v[BK];
+    // this thread's FP32 row (swizzled 16-byte chunks) or, for the
+    // column-staged A tile, column entries
+    auto read_row = [&](const unsigned char *part, float *v) {
+      const float *row = reinterpret_cast<const float *>(part) + p * BK;
+#pragma unroll
+      for (int q = 0; q < BK / 4; ++q) {
+        const float4 x = reinterpret_cast<const float4 *>(row)[q ^ sw];
+        v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+      }
+    };
+    auto read_a = [&](const unsigned char *part, float *v) {
       if (colmode) {
         const float *col = reinterpret_cast<const float *>(part);
 #pragma unroll
         for (int k = 0; k < BK; ++k) v[k] = col[k * 128 + p];
       } else {
-        const float *row = reinterpret_cast<const float *>(part) + p * BK;
-#pragma unroll
-        for (int q = 0; q < BK / 4; ++q) {
-          const float4 x = reinterpret_cast<const float4 *>(row)[q ^ sw];
-          v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
-        }
+        read_row(part, v);
       }
+    };
+    auto split_a = [&](unsigned char *part, const float *v) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) split_store8(v + 8 * c, part, part + A_BYTES, kmajor_off(BM, p, c));
+    };
+    auto split_b = [&](unsigned char *part, const float *v) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) split_store8(v + 8 * c, part, part + B_BYTES, kmajor_off(BN, p, c));
+    };
+    // This group's stages use DG = D / NS ring slots (slot of local stage i:
+    // g0 + NS (i % DG)).  Local stages 0 .. DG - L - 1 are issued up front;
+    // iteration i waits for stage i, splits it in place, hands it to the MMA
+    // warp (full), then refills the slot of local stage i - L -- freed by its
+    // MMAs (empty) -- with local stage i + DG - L, so DG - L - 1 stages stay
+    // in flight while one is split.  con advances alike in every thread
+    // (timeouts included), so the loop condition is uniform across the group.
+    constexpr int D = kStagesP;
+    static_assert(D % NS == 0, "whole slots per group");
+    constexpr int DG = D / NS;
+    constexpr int L = kRefillLag;
+    static_assert(DG - L - 1 >= 1, "a stage in flight while one is split");
+    const int g0 = NS == 2 ? grp : 0;
+    for (int i = 0; i < DG - L; ++i) issue(iss, g0 + NS * i);
+    int li = 0;             // local slot of stage i
+    int rli = DG - L;       // local slot refilled in iteration i: the one of stage i - L
+    uint32_t rphase = 1;    // parity of the empty phase that frees it (fresh: 1)
+    while (con.valid) {
+      cpa_wait<DG - L - 1>();  // this thread's copies of stage i have landed
+      group_sync();            // ... and the whole group's
+      const int slot = g0 + NS * li;
+      float v[BK];
+      if (doA) read_a(a_part(slot), v);
+      else if (p < BN) read_row(b_part(slot), v);
       // every thread has read its FP32 row before the part is overwritten;
       // the same barrier makes the group's exit decision
       if (group_vote_or(abort_sh)) break;
-      if (!isB) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) split_store8(v + 8 * c, part, part + A_BYTES, kmajor_off(BM, p, c));
-      } else if (p < BN) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) split_store8(v + 8 * c, part, part + B_BYTES, kmajor_off(BN, p, c));
+      if (doA) split_a(a_part(slot), v);
+      else if (p < BN) split_b(b_part(slot), v);
+      if (NS == 2) {  // then the B tile of the same stage
+        if (p < BN) read_row(b_part(slot), v);
+        group_sync();
+        if (p < BN) split_b(b_part(slot), v);
       }
       fence_proxy_async();
       mbar_arrive(&full[slot]);
-      if (mbar_wait(&empty[rslot], rphase, spin_limit, suspend)) {
-        issue(iss, rslot);
+      if (mbar_wait(&empty[g0 + NS * rli], rphase, spin_limit, suspend)) {
+        issue(iss, g0 + NS * rli);
       } else {
         abort_sh = 1;  // the group leaves together at the next vote
         cpa_commit();  // keep one copy group per stage
       }
-      if (++rslot == D) { rslot = 0; rphase ^= 1; }
-      if (++slot == D) slot = 0;
-      next(con);
+      if (++rli == DG) { rli = 0; rphase ^= 1; }
+      if (++li == DG) li = 0;
+      adv(con);
     }
     cpa_wait<0>();
   } else if (warp == kMmaWarp) {
