@@ -168,11 +168,13 @@ __device__ inline void mbar_arrive(uint64_t *bar) {
 }
 
 // Persistent, warp-specialized split-operand GEMM.
-//   warps 0-7 (producers): warps 0-3 stage the A tile, warps 4-7 the B tile,
-//     each group cooperatively with cp.async, ring_depth<BN>() - 1 stages
-//     ahead (cp.async.wait_group, then the group's named barrier); thread p
-//     then splits row p of its tile into hi / lo in place, in the UMMA
-//     K-major layout (full[s]: 256 arrivals, empty[s]: tcgen05.commit).
+//   warps 0-7 (producers): two 4-warp groups stage the tiles with cp.async a
+//     few stages ahead (cp.async.wait_group, then the group's named
+//     barrier); thread p then splits row p of a tile into hi / lo in place,
+//     in the UMMA K-major layout (full[s]: one arrival per thread that
+//     splits, empty[s]: tcgen05.commit).  Either group 0 takes the A tile
+//     and group 1 the B tile of every stage, or (prod_streams == 2) each
+//     group takes both tiles of every other stage.
 //   warp 8 lane 0 (MMA issuer): 3 MMAs per k-step into one of two TMEM
 //     accumulators (tfull[a]: commit; tready[a]: one arrival per epilogue
 //     thread once the buffer is drained and preloaded with the next tile's
@@ -200,24 +202,31 @@ constexpr int kThreadsP = kWarps * 32;
 // 128-column tiles, 8 of 24 KB for 64-column ones.
 template <int BN>
 __host__ __device__ constexpr int stage_bytes() { return (128 + BN) * BK * 4; }
-template <int BN>
-__host__ __device__ constexpr int cst_bytes() { return (BN + 4) * 128 * 4; }
+// C tile staging (launches with beta != 0 only)
+template <int BN, bool CIN>
+__host__ __device__ constexpr int cst_bytes() { return CIN ? (BN + 4) * 128 * 4 : 0; }
 constexpr int kSmemPerCta = 232448;  // 227 KB opt-in shared memory per CTA
 constexpr int kStaticSmem = 256;     // the kernel's barriers and flags
 // A group refills the slot of its stage i - kRefillLag after handing stage i
 // to the MMA warp (the MMAs of a stage complete ~0.2 us after their commit).
 constexpr int kRefillLag = 1;
-template <int BN>
+template <int BN, bool CIN>
 __host__ __device__ constexpr int ring_depth() {
-  return (kSmemPerCta - kStaticSmem - 128 - cst_bytes<BN>()) / stage_bytes<BN>();
+  return (kSmemPerCta - kStaticSmem - 128 - cst_bytes<BN, CIN>()) / stage_bytes<BN>();
 }
 // Independent copy / split loops per CTA: on this part one loop with a deep
 // ring reads scattered 128-byte row runs at ~2.8 TB/s over the GPU whatever
 // its depth (cp.async or TMA), two loops per SM at ~3.8-4.2 TB/s.  Two where
-// the ring splits into two halves of at least 3 stages (64-column tiles).
-template <int BN>
+// the ring gives each at least 3 stages (all but 128-column tiles with C
+// staging, which keep one loop over 5 stages); an odd last slot is unused.
+template <int BN, bool CIN>
 __host__ __device__ constexpr int prod_streams() {
-  return (ring_depth<BN>() % 2 == 0 && ring_depth<BN>() / 2 - kRefillLag - 1 >= 1) ? 2 : 1;
+  return ring_depth<BN, CIN>() / 2 - kRefillLag - 1 >= 1 ? 2 : 1;
+}
+// ring slots in use: a multiple of the stream count
+template <int BN, bool CIN>
+__host__ __device__ constexpr int ring_slots() {
+  return ring_depth<BN, CIN>() / prod_streams<BN, CIN>() * prod_streams<BN, CIN>();
 }
 
 __device__ inline void cpa4(void *dst, const void *src, bool ok) {
@@ -334,7 +343,7 @@ __device__ inline void stage_rows_coop(float *dst, int t, const float *base, lon
   }
 }
 
-template <int BN, bool SWAP, typename TC>
+template <int BN, bool SWAP, typename TC, bool CIN>
 __global__ void __launch_bounds__(kThreadsP, 1)
     tc_gemm_persistent(const GemmItem<float, TC> *__restrict__ items,
                        const GemmSeg<float> *__restrict__ segs, int nitems, int mtiles,
@@ -345,7 +354,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
   constexpr int B_BYTES = BN * BK * ELEM;
   constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   static_assert(STAGE_BYTES == stage_bytes<BN>(), "the split fills the FP32 stage exactly");
-  constexpr int kStagesP = ring_depth<BN>();
+  constexpr int kStagesP = ring_slots<BN, CIN>();
   static_assert(kStagesP >= 3, "at least one stage in flight while one is split");
   constexpr int TMEM_COLS = 2 * BN;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -360,7 +369,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
 
   if (tid == 0) {
     for (int s = 0; s < kStagesP; ++s) {
-      mbar_init(&full[s], kProdWarps * 32 / prod_streams<BN>());
+      mbar_init(&full[s], kProdWarps * 32 / prod_streams<BN, CIN>());
       mbar_init(&empty[s], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -438,7 +447,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     // ring (the slots of parity g): two independent copy / split loops per
     // SM.  Thread p owns row p of each tile it splits (rows p >= BN of the B
     // tile do not exist).
-    constexpr int NS = prod_streams<BN>();
+    constexpr int NS = prod_streams<BN, CIN>();
     const int grp = warp >> 2;
     const bool doA = NS == 2 || grp == 0;
     const bool doB = NS == 2 || grp == 1;
@@ -604,7 +613,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(acc * BN);
         const int nst = kstages(it);
-        const uint32_t pre = (it.Cin != nullptr && beta != 0.f) ? 1u : 0u;
+        const uint32_t pre = (CIN && it.Cin != nullptr && beta != 0.f) ? 1u : 0u;
         for (int ks_all = 0; ks_all < nst; ++ks_all) {
           if (!mbar_wait(&full[stage], phase, spin_limit, suspend)) { abort_sh = 1; break; }
           tc_fence_after();
@@ -645,7 +654,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     // memory along j, filled by the row's owner with 16-byte copies).
     constexpr int CSTR = BN + 4;
     auto issue_c = [&](const GemmItem<float, TC> &it, int m0, int n0, int Mu, int Nu) {
-      if (it.Cin != nullptr) {
+      if (CIN && it.Cin != nullptr) {
         const float *cin = reinterpret_cast<const float *>(it.Cin);
         const long long ld = it.ldcin;
         const bool vec = ((reinterpret_cast<uintptr_t>(cin) & 15) == 0) && ((ld & 3) == 0);
@@ -725,6 +734,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     };
     // staged Cin (landed, visible to all epilogue threads) -> TMEM buffer b
     auto preload = [&](const Tile &T, int b) {
+      if constexpr (!CIN) return;
       if (!(T.it.Cin != nullptr && beta != 0.f)) return;
 #pragma unroll 1
       for (int c0 = cbeg; c0 < cend; c0 += 16) {
@@ -784,7 +794,7 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     while (cur.valid) {  // the tile sequence is uniform across the epilogue threads
       const GemmItem<float, TC> &it = cur.it;
       const int m0 = cur.m0, n0 = cur.n0, Mu = cur.Mu, Nu = cur.Nu;
-      const bool live = kstages(it) > 0 || (it.Cin != nullptr && beta != 0.f);
+      const bool live = kstages(it) > 0 || (CIN && it.Cin != nullptr && beta != 0.f);
       const bool ok = mbar_wait(&tfull[acc], aphase, spin_limit, suspend);
       cpa_wait<0>();  // tile j + 2's Cin staged by this thread
       // one barrier: every thread's copies visible, one exit decision for all
@@ -856,11 +866,11 @@ __global__ void __launch_bounds__(kThreadsP, 1)
                  "r"(TMEM_COLS));
 }
 
-template <int BN, bool SWAP, typename TC>
+template <int BN, bool SWAP, typename TC, bool CIN>
 void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int nitems,
                int mu_max, int nu_max, bool trans, float alpha, float beta, cudaStream_t s) {
-  const size_t smem = (size_t)ring_depth<BN>() * stage_bytes<BN>() + cst_bytes<BN>() + 128;
-  raise_smem_limit(reinterpret_cast<const void *>(tc_gemm_persistent<BN, SWAP, TC>), smem);
+  const size_t smem = (size_t)ring_slots<BN, CIN>() * stage_bytes<BN>() + cst_bytes<BN, CIN>() + 128;
+  raise_smem_limit(reinterpret_cast<const void *>(tc_gemm_persistent<BN, SWAP, TC, CIN>), smem);
   const int mt = cdiv(mu_max, BM), nt = cdiv(nu_max, BN);
   const long long total = (long long)nitems * mt * nt;
   int sms = 148;
@@ -871,9 +881,22 @@ void launch_bn(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int
     cudaGetLastError();
   }
   const int grid = (int)std::min<long long>(total, sms);
-  tc_gemm_persistent<BN, SWAP, TC><<<grid, kThreadsP, smem, s>>>(
+  tc_gemm_persistent<BN, SWAP, TC, CIN><<<grid, kThreadsP, smem, s>>>(
       items, segs, nitems, mt, nt, alpha, beta, trans ? 1 : 0, kSuspendNs);
   HODLR_LAUNCH_CHECK();
+}
+
+// tile width by the UMMA N side, C staging only where beta != 0
+template <bool SWAP, typename TC>
+void launch_sw(const GemmItem<float, TC> *items, const GemmSeg<float> *segs, int nitems, int mu,
+               int nu, bool trans, float alpha, float beta, cudaStream_t s) {
+  if (beta != 0.f) {
+    if (nu <= 64) launch_bn<64, SWAP, TC, true>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+    else launch_bn<128, SWAP, TC, true>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+  } else {
+    if (nu <= 64) launch_bn<64, SWAP, TC, false>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+    else launch_bn<128, SWAP, TC, false>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+  }
 }
 
 }  // namespace
@@ -893,11 +916,9 @@ void launch_tc_gemm(const GemmItem<float, TC> *items, const GemmSeg<float> *segs
   const bool swap = max_m < 128 && max_n > max_m;
   const int mu = swap ? max_n : max_m, nu = swap ? max_m : max_n;
   if (swap) {
-    if (nu <= 64) launch_bn<64, true, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
-    else launch_bn<128, true, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+    launch_sw<true, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
   } else {
-    if (nu <= 64) launch_bn<64, false, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
-    else launch_bn<128, false, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
+    launch_sw<false, TC>(items, segs, nitems, mu, nu, trans, alpha, beta, s);
   }
 }
 
