@@ -221,8 +221,11 @@ __host__ __device__ constexpr int ring_depth() {
 // staging, which keep one loop over 5 stages); an odd last slot is unused.
 template <int BN, bool CIN>
 __host__ __device__ constexpr int prod_streams() {
-  return ring_depth<BN, CIN>() / 2 - kRefillLag - 1 >= 1 ? 2 : 1;
+  return ring_depth<BN, CIN>() / 2 >= 2 ? 2 : 1;
 }
+// refill lag of a group with DG ring slots: 1, or 0 where DG = 2 (the group
+// then waits for the MMAs of the stage it has just handed over)
+__host__ __device__ constexpr int refill_lag(int dg) { return dg >= 3 ? kRefillLag : 0; }
 // ring slots in use: a multiple of the stream count
 template <int BN, bool CIN>
 __host__ __device__ constexpr int ring_slots() {
@@ -558,13 +561,13 @@ __global__ void __launch_bounds__(kThreadsP, 1)
     constexpr int D = kStagesP;
     static_assert(D % NS == 0, "whole slots per group");
     constexpr int DG = D / NS;
-    constexpr int L = kRefillLag;
+    constexpr int L = refill_lag(DG);
     static_assert(DG - L - 1 >= 1, "a stage in flight while one is split");
     const int g0 = NS == 2 ? grp : 0;
     for (int i = 0; i < DG - L; ++i) issue(iss, g0 + NS * i);
     int li = 0;             // local slot of stage i
-    int rli = DG - L;       // local slot refilled in iteration i: the one of stage i - L
-    uint32_t rphase = 1;    // parity of the empty phase that frees it (fresh: 1)
+    int rli = (DG - L) % DG;       // local slot refilled in iteration i: the one of stage i - L
+    uint32_t rphase = L > 0 ? 1 : 0;  // parity of the empty phase that frees it (fresh: 1)
     while (con.valid) {
       cpa_wait<DG - L - 1>();  // this thread's copies of stage i have landed
       group_sync();            // ... and the whole group's
