@@ -117,11 +117,21 @@ __device__ inline void nn_rows_unit(const GemmItem<float, float> *__restrict__ i
 #pragma unroll
       for (int k = 0; k < kRowKC; ++k)
         a[k] = (k < kc) ? ldg_unit<CG>(ap + (long long)k * sg.lda) : 0.f;
-      __syncthreads();  // the previous chunk's B reads are done
-      for (int e = tid; e < kRowKC * NC; e += kRowThreads) {
+      // ... and this thread's share of the chunk's B block, in flight with them
+      constexpr int kBPer = kRowKC * NC / kRowThreads;
+      static_assert(kBPer * kRowThreads == kRowKC * NC, "whole B block per pass");
+      float bv[kBPer];
+#pragma unroll
+      for (int j = 0; j < kBPer; ++j) {
+        const int e = tid + j * kRowThreads;
         const int k = e % kRowKC, n = e / kRowKC;
-        Bs[k * NC + n] =
-            (k < kc && n < N) ? ldg_unit<CG>(sg.B + (k0 + k) + (long long)n * sg.ldb) : 0.f;
+        bv[j] = (k < kc && n < N) ? ldg_unit<CG>(sg.B + (k0 + k) + (long long)n * sg.ldb) : 0.f;
+      }
+      __syncthreads();  // the previous chunk's B reads are done
+#pragma unroll
+      for (int j = 0; j < kBPer; ++j) {
+        const int e = tid + j * kRowThreads;
+        Bs[(e % kRowKC) * NC + e / kRowKC] = bv[j];
       }
       __syncthreads();
 #pragma unroll
@@ -138,14 +148,22 @@ __device__ inline void nn_rows_unit(const GemmItem<float, float> *__restrict__ i
     }
   }
   if (!live) return;
+  // all of the row's Cin values before any store: C may be Cin (in-place
+  // d -= u eta), so loads issued between the stores would each wait for the
+  // one before
+  float cin[NC];
+  if (it.Cin) {
+#pragma unroll
+    for (int n = 0; n < NC; ++n) {
+      const float *cp = it.Cin + row + (long long)n * it.ldcin;
+      cin[n] = n < N ? (CG ? __ldcg(cp) : *cp) : 0.f;
+    }
+  }
 #pragma unroll
   for (int n = 0; n < NC; ++n) {
     if (n >= N) break;
     float v = alpha * acc[n];
-    if (it.Cin) {
-      const float *cp = it.Cin + row + (long long)n * it.ldcin;
-      v += beta * (CG ? __ldcg(cp) : *cp);
-    }
+    if (it.Cin) v += beta * cin[n];
     it.C[row + (long long)n * it.ldc] = v;
   }
 }
@@ -260,6 +278,16 @@ __device__ inline void tn2_unit(const GemmItem<T, T> *__restrict__ items,
     cp.next(KC);
   }
   cpa_wait<0>();
+  // every Cin value before any store (C may be Cin)
+  T cin[2][4];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gm = m0 + mm + 32 * h, gn = n0 + n4 + j;
+      const T *cp = it.Cin ? it.Cin + gm + (long long)gn * it.ldcin : nullptr;
+      cin[h][j] = (cp && gm < it.M && gn < it.N) ? (CG ? __ldcg(cp) : *cp) : T(0);
+    }
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int gm = m0 + mm + 32 * h;
@@ -269,10 +297,7 @@ __device__ inline void tn2_unit(const GemmItem<T, T> *__restrict__ items,
       const int gn = n0 + n4 + j;
       if (gn >= it.N) break;
       T v = alpha * acc[h][j];
-      if (it.Cin) {
-        const T *cp = it.Cin + gm + (long long)gn * it.ldcin;
-        v += beta * (CG ? __ldcg(cp) : *cp);
-      }
+      if (it.Cin) v += beta * cin[h][j];
       it.C[gm + (long long)gn * it.ldc] = v;
     }
   }

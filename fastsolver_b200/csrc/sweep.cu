@@ -84,10 +84,12 @@ __device__ bool grid_sync(unsigned *bar, unsigned &gen, long long limit) {
   return s_ok != 0;
 }
 
-// 4 CTAs (16 warps) per SM: the units need ~128 registers per thread; a
-// tighter register bound makes them spill
+// 3 CTAs (12 warps) per SM: the units keep a chunk of A, their share of B
+// and a row's Cin values in registers (up to 168 per thread); measured at
+// N = 262144 (m = 16) the same sweep time as 4 CTAs per SM, where the
+// 128-register bound makes them spill
 template <int NC>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 3)
     sweep_levels_kernel(const SweepLevel *__restrict__ levels, int nlevels, unsigned *bar) {
   extern __shared__ __align__(16) unsigned char smem[];
   const long long limit = g_sweep_spin_limit > 0 ? g_sweep_spin_limit : kSweepSpinDefault;
