@@ -111,12 +111,19 @@ __global__ void __launch_bounds__(NT)
   for (int j = 0; j < TN; ++j) {
     const int gn = n0 + tc * TN + j;
     if (gn >= it.N) continue;
+    // the column's Cin values before its stores (C may alias Cin)
+    TC cin[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int gm = m0 + tr * 4 + i;
+      cin[i] = (it.Cin && gm < it.M) ? it.Cin[gm + (long long)gn * it.ldcin] : TC(0);
+    }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int gm = m0 + tr * 4 + i;
       if (gm >= it.M) continue;
       TACC v = alpha * acc[i][j];
-      if (it.Cin) v += beta * TACC(it.Cin[gm + (long long)gn * it.ldcin]);
+      if (it.Cin) v += beta * TACC(cin[i]);
       it.C[gm + (long long)gn * it.ldc] = TC(v);
     }
   }
@@ -177,11 +184,16 @@ __global__ void __launch_bounds__(NT)
     }
   }
   if (row < it.M) {
+    // the row's Cin values before its stores (C may alias Cin)
+    TC cin[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+      cin[c] = (it.Cin && c < it.N) ? it.Cin[row + (long long)c * it.ldcin] : TC(0);
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       if (c >= it.N) break;
       TACC v = alpha * acc[c];
-      if (it.Cin) v += beta * TACC(it.Cin[row + (long long)c * it.ldcin]);
+      if (it.Cin) v += beta * TACC(cin[c]);
       it.C[row + (long long)c * it.ldc] = TC(v);
     }
   }

@@ -153,12 +153,23 @@ __global__ void __launch_bounds__(kSkThreads)
   for (int h = 0; h < 2; ++h) {
     const int row = row0 + tid + h * kSkThreads;
     if (row < it.M) {
+      static_assert(NC % 8 == 0, "whole column groups");
+      // per 8 columns: their Cin values before their stores (C may alias
+      // Cin, so a load after a store would wait for it)
 #pragma unroll
-      for (int n = 0; n < NC; ++n) {
-        if (n >= N) break;
-        T v = alpha * (h ? acc1[n] : acc0[n]);
-        if (it.Cin) v += beta * it.Cin[row + (long long)n * it.ldcin];
-        it.C[row + (long long)n * it.ldc] = v;
+      for (int n8 = 0; n8 < NC; n8 += 8) {
+        T cin[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          cin[u] = (it.Cin && n8 + u < N) ? it.Cin[row + (long long)(n8 + u) * it.ldcin] : T(0);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int n = n8 + u;
+          if (n >= N) break;
+          T v = alpha * (h ? acc1[n] : acc0[n]);
+          if (it.Cin) v += beta * cin[u];
+          it.C[row + (long long)n * it.ldc] = v;
+        }
       }
     }
   }
@@ -287,8 +298,20 @@ __global__ void __launch_bounds__(kSkThreads, 2)
     cp.next(KT);
   }
   cpa_wait<0>();
+  // per 16-row fragment: its Cin values before its stores (C may alias Cin,
+  // so a load after a store would wait for it)
 #pragma unroll
-  for (int mt = 0; mt < 4; ++mt)
+  for (int mt = 0; mt < 4; ++mt) {
+    double cin[NT8][4];
+#pragma unroll
+    for (int nt = 0; nt < NT8; ++nt)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int row = row0 + wrow + mt * 16 + g + (v >> 1) * 8;
+        const int c = nt * 8 + 2 * t + (v & 1);
+        cin[nt][v] = (it.Cin && row < it.M && c < N) ? it.Cin[row + (n0 + c) * (long long)it.ldcin]
+                                                      : 0.0;
+      }
 #pragma unroll
     for (int nt = 0; nt < NT8; ++nt)
 #pragma unroll
@@ -298,10 +321,11 @@ __global__ void __launch_bounds__(kSkThreads, 2)
         if (row < it.M && c < N) {
           const long long col = n0 + c;
           double val = alpha * acc[mt][nt][v];
-          if (it.Cin) val += beta * it.Cin[row + col * it.ldcin];
+          if (it.Cin) val += beta * cin[nt][v];
           it.C[row + col * it.ldc] = val;
         }
       }
+  }
 }
 
 // TN: C (64 x 16 block of an item, over all K) = beta Cin + alpha sum_s A_s^T B_s
@@ -379,6 +403,16 @@ __global__ void __launch_bounds__(kTNThreads)
     cp.next(KC);
   }
   cpa_wait<0>();
+  // every Cin value before any store (C may alias Cin)
+  double cin[2][4];
+#pragma unroll
+  for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int gm = m0 + warp * 16 + g + (v >> 1) * 8;
+      const int gn = n0 + nt * 8 + 2 * t + (v & 1);
+      cin[nt][v] = (it.Cin && gm < it.M && gn < it.N) ? it.Cin[gm + (long long)gn * it.ldcin] : 0.0;
+    }
 #pragma unroll
   for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
@@ -387,7 +421,7 @@ __global__ void __launch_bounds__(kTNThreads)
       const int gn = n0 + nt * 8 + 2 * t + (v & 1);
       if (gm < it.M && gn < it.N) {
         double val = alpha * acc[nt][v];
-        if (it.Cin) val += beta * it.Cin[gm + (long long)gn * it.ldcin];
+        if (it.Cin) val += beta * cin[nt][v];
         it.C[gm + (long long)gn * it.ldc] = val;
       }
     }
