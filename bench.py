@@ -676,7 +676,7 @@ def main():
     bytes_per_launch = upd_bytes / max(n_upd, 1)
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
     traffic = profile_traffic(os.path.join(ROOT, "profiles", "leaf_update_gemm_n262144.md"))
-    roofline = {"bound": "hbm", "kernel": "tc_gemm_persistent<128,false> (leaf trailing update)",
+    roofline = {"bound": "hbm", "kernel": "tc_gemm_persistent<128,false,float,true> (leaf trailing update)",
                 "achieved": achieved, "peak": pk["hbm"], "unit": "GB/s",
                 "frac": achieved / pk["hbm"], "traffic": traffic,
                 "algorithmic_bytes_per_launch": bytes_per_launch,
