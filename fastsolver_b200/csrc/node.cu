@@ -19,8 +19,9 @@
 // (form 1, the 2r x 2r system [[V0Tu0, I], [I, V1Tu1]] of the leaf-internal
 // branch: M is that matrix's inverse).  node_factor_kernel forms M once per
 // node -- one CTA per node, S^{-1} by Gauss-Jordan elimination with partial
-// pivoting in shared memory (pivot = largest |a|, lowest row on ties, as
-// LAPACK's idamax), the three products from shared memory and L2 -- and the
+// pivoting (pivot = largest |a|, lowest row on ties, as LAPACK's idamax; in
+// registers for s <= 64, in shared memory above), the three products from
+// shared memory and L2 -- and the
 // solver applies M to every column block as one batched GEMM per level (the
 // same engine as the reduce and broadcast), for the fused pass and for every
 // later solve with the same factors.  INFO > 0 reports an exactly zero pivot
@@ -136,6 +137,102 @@ __device__ inline void node_product_dmma(int rows, int cols, int K, double alpha
   }
 }
 
+// Gauss-Jordan elimination with implicit row interchanges of the s x s
+// matrix A (s <= 64, row-major in shared memory, row stride lda), the same
+// steps as the shared-memory elimination of node_factor_kernel but on
+// registers: warp w holds rows 4w .. 4w + 3, lane (row, g) (g = lane % 8)
+// columns g, g + 8, ..., g + 56 of its row.  Per column k every warp finds
+// its best candidate (largest |a| among the rows not yet pivotal, lowest
+// current position on ties, as idamax after LAPACK's interchanges) and the
+// candidate row's 8 lanes publish the row (double-buffered); one barrier;
+// every warp combines the 16 candidates and eliminates column k from its rows
+// with the published (unscaled) pivot row, while the pivot row's lanes scale
+// their own values.  Measured on B200 with s = 64: the shared-memory form
+// spent ~3.5 k cycles per column, mostly re-reading and re-writing the whole
+// matrix in shared memory.  On return A holds the eliminated matrix (the
+// input of the inverse's gather), piv[k] the interchange of step k, at[i] the
+// storage row at final position i, *s_info the first zero pivot (1-based) or
+// 0.  Every thread of the CTA calls it.
+__device__ inline void gj_registers(double *A, int lda, int s, int *piv, int *at, int *s_info) {
+  constexpr int NWG = kNodeWarps;
+  __shared__ __align__(16) double wrow[2][NWG][64];
+  __shared__ double wval[2][NWG];
+  __shared__ int wpos[2][NWG], wcode[2][NWG];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i = 4 * warp + (lane >> 3);  // this lane's row
+  const int g = lane & 7;                // its column group
+  const bool rowok = i < s;
+  double a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int c = g + 8 * j;
+    a[j] = (rowok && c < s) ? A[i * lda + c] : 0.0;
+  }
+  int pos = i;          // current position of row i (LAPACK interchange order)
+  bool used = !rowok;   // row already pivotal (or absent)
+  int info = 0;
+  for (int k = 0; k < s; ++k) {
+    const int slot = k & 1, kg = k & 7, kj = k >> 3;
+    // A[i][k], held by lane (row, kg) at register kj
+    double mine = a[0];
+#pragma unroll
+    for (int j = 1; j < 8; ++j)
+      if (j == kj) mine = a[j];
+    const double aik = __shfl_sync(0xffffffffu, mine, (lane & ~7) | kg);
+    double best = 0.0;
+    int bp = 0x7fffffff, code = -1;
+    if (g == kg && !used) {
+      const double av = fabs(aik);
+      if (av == av) { best = av; bp = pos; code = i; }  // NaN is never a candidate
+    }
+    int wl;
+    warp_argmax_f64(best, bp, code, wl);
+    if (code >= 0 && i == code) {  // the warp's candidate row publishes itself
+#pragma unroll
+      for (int j = 0; j < 8; ++j) wrow[slot][warp][g + 8 * j] = a[j];
+    }
+    if (lane == 0) { wval[slot][warp] = best; wpos[slot][warp] = bp; wcode[slot][warp] = code; }
+    __syncthreads();
+    double pb = 0.0;
+    int pp = 0x7fffffff, pc = -1, pw = 0;
+    if (lane < NWG) { pb = wval[slot][lane]; pp = wpos[slot][lane]; pc = wcode[slot][lane]; }
+    warp_argmax_f64(pb, pp, pc, pw);  // pw: the winning warp
+    const double pk = pc >= 0 ? wrow[slot][pw][k] : 0.0;
+    if (pk == 0.0) {  // exactly singular (or a NaN column): INFO = k + 1, uniform
+      info = k + 1;
+      break;
+    }
+    if (tid == 0) piv[k] = pp;
+    const double rinv = 1.0 / pk;
+    if (rowok) {
+      if (i == pc) {
+        pos = k;
+        used = true;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = (g + 8 * j == k) ? rinv : a[j] * rinv;
+      } else {
+        if (pos == k) pos = pp;
+        const double f = aik * rinv;
+        const double *prow = wrow[slot][pw];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int c = g + 8 * j;
+          a[j] = (c == k) ? -f : a[j] - f * prow[c];
+        }
+      }
+    }
+  }
+  if (rowok) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int c = g + 8 * j;
+      if (c < s) A[i * lda + c] = a[j];
+    }
+    if (g == 0 && info == 0) at[pos] = i;
+  }
+  if (tid == 0) *s_info = info;
+}
+
 template <typename TW, typename TE, int RL>
 __global__ void __launch_bounds__(kNodeThreads)
     node_factor_kernel(const NodeTask<TW, TE> *tasks, int form, int max_s, int max_r, int stage,
@@ -185,104 +282,108 @@ __global__ void __launch_bounds__(kNodeThreads)
   }
   __syncthreads();
 
-  // ---- Gauss-Jordan with implicit row interchanges, one barrier per column.
-  // Rows never move; every warp finds the pivot of column k itself (largest
-  // |a| among the rows not yet pivotal, lowest current position on ties, as
-  // idamax after LAPACK's interchanges) and keeps identical copies of the
-  // rows' current positions.  Warp w eliminates column k from rows w, w + kNodeWarps,
-  // ... with the (unscaled) pivot row; the pivot row itself is scaled by its
-  // owner at the start of the next step, when nobody else reads it.
-  // RL: rows (and columns) per lane, ceil(max_s / 32)
-  int posr[RL];
-  bool usedr[RL];
-#pragma unroll
-  for (int t = 0; t < RL; ++t) {
-    const int row = lane + 32 * t;
-    posr[t] = row;
-    usedr[t] = row >= s;
-  }
-  int prevp = -1, prevk = -1;
-  double prevr = 0.0;
-  auto scale_prev = [&]() {
-    if (prevp >= 0 && (prevp % kNodeWarps) == warp) {
-      double *Ap = A + prevp * lda;
-      for (int c = lane; c < s; c += 32) Ap[c] = (c == prevk) ? prevr : Ap[c] * prevr;
-    }
-  };
-  for (int k = 0; k < s; ++k) {
-    scale_prev();
-    // the owner warp's lanes wrote the previous pivot row, whose column k the
-    // same warp reads below (Ai[k] of its rows): order those accesses
-    __syncwarp();
-    double best = 0.0;
-    int bp = 0x7fffffff, code = -1;
-#pragma unroll
+  if constexpr (RL <= 2) {
+    gj_registers(A, lda, s, piv, at, &s_info);
+  } else {
+    // ---- Gauss-Jordan with implicit row interchanges, one barrier per column.
+    // Rows never move; every warp finds the pivot of column k itself (largest
+    // |a| among the rows not yet pivotal, lowest current position on ties, as
+    // idamax after LAPACK's interchanges) and keeps identical copies of the
+    // rows' current positions.  Warp w eliminates column k from rows w, w + kNodeWarps,
+    // ... with the (unscaled) pivot row; the pivot row itself is scaled by its
+    // owner at the start of the next step, when nobody else reads it.
+    // RL: rows (and columns) per lane, ceil(max_s / 32)
+    int posr[RL];
+    bool usedr[RL];
+  #pragma unroll
     for (int t = 0; t < RL; ++t) {
       const int row = lane + 32 * t;
-      if (row < s && !usedr[t]) {
-        const double av = fabs(A[row * lda + k]);
-        if (av == av && (bp == 0x7fffffff || av > best || (av == best && posr[t] < bp))) {
-          best = av; bp = posr[t]; code = row;
+      posr[t] = row;
+      usedr[t] = row >= s;
+    }
+    int prevp = -1, prevk = -1;
+    double prevr = 0.0;
+    auto scale_prev = [&]() {
+      if (prevp >= 0 && (prevp % kNodeWarps) == warp) {
+        double *Ap = A + prevp * lda;
+        for (int c = lane; c < s; c += 32) Ap[c] = (c == prevk) ? prevr : Ap[c] * prevr;
+      }
+    };
+    for (int k = 0; k < s; ++k) {
+      scale_prev();
+      // the owner warp's lanes wrote the previous pivot row, whose column k the
+      // same warp reads below (Ai[k] of its rows): order those accesses
+      __syncwarp();
+      double best = 0.0;
+      int bp = 0x7fffffff, code = -1;
+  #pragma unroll
+      for (int t = 0; t < RL; ++t) {
+        const int row = lane + 32 * t;
+        if (row < s && !usedr[t]) {
+          const double av = fabs(A[row * lda + k]);
+          if (av == av && (bp == 0x7fffffff || av > best || (av == best && posr[t] < bp))) {
+            best = av; bp = posr[t]; code = row;
+          }
         }
       }
-    }
-    int wl;
-    warp_argmax_f64(best, bp, code, wl);
-    const int p = code, pp = bp;
-    const double pk = p >= 0 ? A[p * lda + k] : 0.0;
-    if (pk == 0.0) {  // exactly singular (or a NaN column): INFO = k + 1, uniform
-      if (tid == 0) s_info = k + 1;
-      break;
-    }
-#pragma unroll
-    for (int t = 0; t < RL; ++t) {
-      const int row = lane + 32 * t;
-      if (row == p) { posr[t] = k; usedr[t] = true; }
-      else if (posr[t] == k) posr[t] = pp;
-    }
-    if (tid == 0) piv[k] = pp;
-    const double rinv = 1.0 / pk;
-    double prow[RL];
-#pragma unroll
-    for (int u = 0; u < RL; ++u) {
-      const int c = lane + 32 * u;
-      prow[u] = c < s ? A[p * lda + c] : 0.0;
-    }
-    // this warp's rows i = warp, warp + kNodeWarps, ...: all multipliers are
-    // read before any lane writes column k (one __syncwarp), so the row
-    // updates are independent and overlap
-    constexpr int RW = (kMaxNodeS + kNodeWarps - 1) / kNodeWarps;
-    double fr[RW];
-#pragma unroll
-    for (int jj = 0; jj < RW; ++jj) {
-      const int i = warp + kNodeWarps * jj;
-      fr[jj] = (i < s && i != p) ? A[i * lda + k] * rinv : 0.0;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int jj = 0; jj < RW; ++jj) {
-      const int i = warp + kNodeWarps * jj;
-      if (i >= s || i == p) continue;
-      double *Ai = A + i * lda;
-#pragma unroll
+      int wl;
+      warp_argmax_f64(best, bp, code, wl);
+      const int p = code, pp = bp;
+      const double pk = p >= 0 ? A[p * lda + k] : 0.0;
+      if (pk == 0.0) {  // exactly singular (or a NaN column): INFO = k + 1, uniform
+        if (tid == 0) s_info = k + 1;
+        break;
+      }
+  #pragma unroll
+      for (int t = 0; t < RL; ++t) {
+        const int row = lane + 32 * t;
+        if (row == p) { posr[t] = k; usedr[t] = true; }
+        else if (posr[t] == k) posr[t] = pp;
+      }
+      if (tid == 0) piv[k] = pp;
+      const double rinv = 1.0 / pk;
+      double prow[RL];
+  #pragma unroll
       for (int u = 0; u < RL; ++u) {
         const int c = lane + 32 * u;
-        if (c < s) Ai[c] = (c == k) ? -fr[jj] : Ai[c] - fr[jj] * prow[u];
+        prow[u] = c < s ? A[p * lda + c] : 0.0;
       }
+      // this warp's rows i = warp, warp + kNodeWarps, ...: all multipliers are
+      // read before any lane writes column k (one __syncwarp), so the row
+      // updates are independent and overlap
+      constexpr int RW = (kMaxNodeS + kNodeWarps - 1) / kNodeWarps;
+      double fr[RW];
+  #pragma unroll
+      for (int jj = 0; jj < RW; ++jj) {
+        const int i = warp + kNodeWarps * jj;
+        fr[jj] = (i < s && i != p) ? A[i * lda + k] * rinv : 0.0;
+      }
+      __syncwarp();
+  #pragma unroll
+      for (int jj = 0; jj < RW; ++jj) {
+        const int i = warp + kNodeWarps * jj;
+        if (i >= s || i == p) continue;
+        double *Ai = A + i * lda;
+  #pragma unroll
+        for (int u = 0; u < RL; ++u) {
+          const int c = lane + 32 * u;
+          if (c < s) Ai[c] = (c == k) ? -fr[jj] : Ai[c] - fr[jj] * prow[u];
+        }
+      }
+      prevp = p;
+      prevk = k;
+      prevr = rinv;
+      __syncthreads();
     }
-    prevp = p;
-    prevk = k;
-    prevr = rinv;
-    __syncthreads();
-  }
-  __syncthreads();  // s_info (set on the singular break) visible to all
-  if (s_info == 0) scale_prev();
-  // at[i]: the storage row at final position i (every warp holds the same posr)
-  if (warp == 0) {
-#pragma unroll
-    for (int t = 0; t < RL; ++t) {
-      const int row = lane + 32 * t;
-      if (row < s) at[posr[t]] = row;
+    __syncthreads();  // s_info (set on the singular break) visible to all
+    if (s_info == 0) scale_prev();
+    // at[i]: the storage row at final position i (every warp holds the same posr)
+    if (warp == 0) {
+  #pragma unroll
+      for (int t = 0; t < RL; ++t) {
+        const int row = lane + 32 * t;
+        if (row < s) at[posr[t]] = row;
+      }
     }
   }
   __syncthreads();

@@ -96,6 +96,32 @@ def test_batch_graph_replay_new_rhs(fs, oracle, cuda):
             _check(oracle, s, h, cfg[1], r, stream=st)
 
 
+@pytest.mark.parametrize("order", ["large_leaves_first", "small_leaves_first"])
+def test_batch_graph_replay_leaf_groups_both_orders(fs, oracle, cuda, order):
+    """Two leaf groups of the 17..32-column apply class (leaves up to 1024
+    rows and up to 512 rows, different dynamic shared memory) captured in
+    one graph, built in either order, then replayed with new right-hand
+    sides: the kernel's shared-memory limit only ever rises, so every
+    captured node can launch on replay."""
+    import torch
+    cfgs = [(9001, 32, 24, 1024), (12000, 32, 40, 512)]
+    if order == "small_leaves_first":
+        cfgs = cfgs[::-1]
+    pairs = [_load(fs, oracle, *cfg, seed=300 + i) for i, cfg in enumerate(cfgs)]
+    batch = fs.SystemBatch([h for _, h in pairs])
+    st = torch.cuda.Stream()
+    rng = np.random.default_rng(11)
+    for trial in range(3):
+        for (s, h), cfg in zip(pairs, cfgs):
+            s.B = np.asfortranarray(rng.standard_normal((cfg[0], cfg[1])))
+            h.set_rhs(s.B, stream=st)
+        it, rr = batch.solve_refined(tol=1e-12, maxiter=10, stream=st)
+        st.synchronize()
+        for (s, h), cfg, r in zip(pairs, cfgs, rr):
+            _check(oracle, s, h, cfg[1], r, stream=st)
+    batch.close()
+
+
 def test_batch_leaves_systems_factored(fs, oracle, cuda):
     """After a batch solve every system holds its mixed factors: a plain
     hodlr_solve of a new RHS applies them (FP32 accuracy, no refinement)."""
