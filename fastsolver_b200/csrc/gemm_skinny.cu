@@ -455,8 +455,8 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
     return;
   }
   if (trans) {
-    constexpr int TM = 64, TN = 16, KC = 32, LDK = KC + 16 / sizeof(T);
-    const size_t smem = (size_t)kSkStages * (TM + TN) * LDK * sizeof(T);
+    constexpr int TM = 64, TN = 16;
+    const size_t smem = tn2_smem_bytes<T>();
     raise_smem_limit(reinterpret_cast<const void *>(skinny_tn2_kernel<T>), smem);
     dim3 grid(nitems, cdiv(max_m, TM), cdiv(max_n, TN));
     skinny_tn2_kernel<T><<<grid, kTNThreads, smem, s>>>(items, segs, alpha, beta);

@@ -88,7 +88,10 @@ struct Vec {
 constexpr int kRowThreads = 128;
 
 template <int NC>
-__host__ __device__ constexpr int nn_rows_kc() { return NC > 16 ? 16 : 32; }  // k-values in flight per thread
+// k-values in flight per thread (a whole K = 64 chunk for up to 16 columns
+// made the persistent sweep spill and run slower: 2.02 -> 2.12 ms for two
+// sweeps at N = 262144)
+__host__ __device__ constexpr int nn_rows_kc() { return NC > 16 ? 16 : 32; }
 
 // One CTA (kRowThreads threads) computes rows [rb * kRowThreads, ...) of item
 // `item`; Bs holds nn_rows_kc<NC>() * NC floats.  CTA-uniform.

@@ -156,7 +156,9 @@ __global__ void __launch_bounds__(kThreads, 3)
 }
 
 size_t sweep_smem() {
-  return std::max(tn2_smem_bytes<float>(), (size_t)nn_rows_kc<8>() * 32 * sizeof(float));
+  const size_t rows_b = std::max({nn_rows_kc<8>() * 8, nn_rows_kc<16>() * 16, nn_rows_kc<32>() * 32}) *
+                       sizeof(float);
+  return std::max(tn2_smem_bytes<float>(), rows_b);
 }
 
 template <int NC>
