@@ -14,7 +14,9 @@ device.  One step = one solve of that system with its whole RHS block:
   fp64_gpu  the plain FP64 path (the fused factor+solve of the reference's
             bfs_solve), same system, timed the same way
   e2e       `value`'s solve through the public API with the system in pinned
-            host memory: H2D of D, U, V, b and D2H of x inside every step
+            host memory: one hodlr_solve_refined_host call per step (H2D of
+            D, U, V, b, with V's copy under the leaf factorization, the
+            refined solve, D2H of x)
   --impl reference: the CPU oracle (a restatement of the reference's
             Legion+LAPACK path with OpenBLAS, all host threads) on the same
             workload, printed as the reference arm.
@@ -623,12 +625,14 @@ def main():
         from fastsolver_b200._lib import call
         import ctypes
 
+        it_e, rr_e = ctypes.c_int(), ctypes.c_double()
+
         def e2e_step():
-            call("hodlr_set_matrix", h.handle, Dp.data_ptr(), N, Up.data_ptr(), N,
-                 Vp.data_ptr(), N, 1, stream.cuda_stream)
-            call("hodlr_set_rhs", h.handle, Bp.data_ptr(), N, 1, stream.cuda_stream)
-            mixed_step()
-            call("hodlr_get_solution", h.handle, xout.data_ptr(), N, 1, stream.cuda_stream)
+            # one host-to-host call: D, U, V, b in from pinned memory (V's copy
+            # under the leaf factorization), refined solve, x out
+            call("hodlr_solve_refined_host", h.handle, Dp.data_ptr(), N, Up.data_ptr(), N,
+                 Vp.data_ptr(), N, Bp.data_ptr(), N, xout.data_ptr(), N, fs.PREC_MIXED, TOL, 10,
+                 ctypes.byref(it_e), ctypes.byref(rr_e), stream.cuda_stream)
 
         e2e_step()
         torch.cuda.synchronize()
@@ -643,7 +647,7 @@ def main():
         h2d = (Dp.numel() + Up.numel() + Vp.numel() + Bp.numel()) * 8
         e2e = {"value": replica_value(ms_e2e, ws), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(xout.numel() * 8), "ms_per_step": ms_e2e,
-               "steps": ksteps}
+               "steps": ksteps, "relres": rr_e.value, "refine_sweeps": it_e.value}
 
     if rank != 0:
         if dist is not None:

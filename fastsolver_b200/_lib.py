@@ -72,6 +72,8 @@ _SIGS = {
     "hodlr_factor": [_vp, _i, _vp],
     "hodlr_solve": [_vp, _vp],
     "hodlr_solve_refined": [_vp, _i, _d, _i, _ip, _dp, _vp],
+    "hodlr_solve_refined_host": [_vp, _vp, _ll, _vp, _ll, _vp, _ll, _vp, _ll, _vp, _ll, _i, _d,
+                                 _i, _ip, _dp, _vp],
     "hodlr_matvec": [_vp, _vp, _ll, _vp, _ll, _i, _vp],
     "hodlr_relres": [_vp, _dp, _vp],
     "hodlr_get_solution": [_vp, _vp, _ll, _i, _vp],

@@ -845,13 +845,27 @@ int hodlr_solve(hodlr_system h, hodlr_stream_t stream) {
 }
 
 // The refined solve of one system on stream s (see hodlr_solve_refined).
+// With v_ready, the mixed factor pass runs as two segments, the leaf
+// factorization and the tree levels, and s waits for v_ready (V on the
+// device) between them.
 static int refined_body(System &S, int precision, double tol, int maxiter, int *iters,
-                        double *relres, cudaStream_t s) {
+                        double *relres, cudaStream_t s, cudaEvent_t v_ready = nullptr) {
   const long long N = S.N;
   const size_t nm = (size_t)N * S.m;
   // two replayable segments: factor pass + residual, and one refinement
   // sweep + residual (captured as CUDA graphs on the first call)
-  if (precision == HODLR_PREC_MIXED) {
+  if (precision == HODLR_PREC_MIXED && v_ready) {
+    S.ensure_mixed();
+    S.run_graph(S.g_factor32_leaves, s, [&]() { S.run_factor32_part(kPathLeaves, s); });
+    HODLR_CUDA_TRY(cudaStreamWaitEvent(s, v_ready, 0));
+    S.run_graph(S.g_factor32_levels, s, [&]() {
+      S.run_factor32_part(kPathLevels, s);
+      launch_convert2d<float, double>(S.X32.p, N, S.Xsol.p, N, N, S.m, s);
+      S.relres_enqueue(s);
+    });
+    S.factored = HODLR_PREC_MIXED;
+    S.factored_form = 0;
+  } else if (precision == HODLR_PREC_MIXED) {
     S.ensure_mixed();
     S.run_graph(S.g_factor32, s, [&]() {
       S.run_factor32(s);
@@ -909,6 +923,60 @@ int hodlr_solve_refined(hodlr_system h, int precision, double tol, int maxiter, 
   if (maxiter < 0) return -4;
   return guarded([&]() -> int {
     return refined_body(h->sys, precision, tol, maxiter, iters, relres, as_stream(stream));
+  });
+}
+
+int hodlr_solve_refined_host(hodlr_system h, const double *D, long long ldd, const double *U,
+                             long long ldu, const double *V, long long ldv, const double *B,
+                             long long ldb, double *X, long long ldx, int precision, double tol,
+                             int maxiter, int *iters, double *relres, hodlr_stream_t stream) {
+  if (!h) return -1;
+  System &S = h->sys;
+  if (!D) return -2;
+  if (ldd < S.N) return -3;
+  if (S.vc > 0 && !U) return -4;
+  if (S.vc > 0 && ldu < S.N) return -5;
+  if (S.vc > 0 && !V) return -6;
+  if (S.vc > 0 && ldv < S.N) return -7;
+  if (!B) return -8;
+  if (ldb < S.N) return -9;
+  if (!X) return -10;
+  if (ldx < S.N) return -11;
+  if (precision != HODLR_PREC_FP64 && precision != HODLR_PREC_MIXED) return -12;
+  if (!(tol >= 0.0)) return -13;
+  if (maxiter < 0) return -14;
+  return guarded([&]() -> int {
+    cudaStream_t s = as_stream(stream);
+    // no return while a copy may still read the caller's buffers
+    struct DrainLane {
+      cudaStream_t st = nullptr;
+      ~DrainLane() {
+        if (st) cudaStreamSynchronize(st);
+      }
+    } drain;
+    copy2d(S.D.p, S.N, D, ldd, S.N, S.nmax, 1, s);
+    copy2d(S.B.p, S.N, B, ldb, S.N, S.m, 1, s);
+    if (S.vc > 0) copy2d(S.U.p, S.N, U, ldu, S.N, S.vc, 1, s);
+    S.factored = -1;
+    cudaEvent_t v_ready = nullptr;
+    if (S.vc > 0 && precision == HODLR_PREC_MIXED) {
+      // V is first read by the tree levels: its copy follows the others on
+      // the copy lane, under the leaf factorization
+      S.lane.ensure();
+      drain.st = S.lane.stream;
+      HODLR_CUDA_TRY(cudaEventRecord(S.lane.inputs, s));
+      HODLR_CUDA_TRY(cudaStreamWaitEvent(S.lane.stream, S.lane.inputs, 0));
+      copy2d(S.V.p, S.N, V, ldv, S.N, S.vc, 1, S.lane.stream);
+      HODLR_CUDA_TRY(cudaEventRecord(S.lane.v, S.lane.stream));
+      v_ready = S.lane.v;
+    } else if (S.vc > 0) {
+      copy2d(S.V.p, S.N, V, ldv, S.N, S.vc, 1, s);
+    }
+    const int rc = refined_body(S, precision, tol, maxiter, iters, relres, s, v_ready);
+    HODLR_CUDA_TRY(cudaMemcpy2DAsync(X, sizeof(double) * ldx, S.Xsol.p, sizeof(double) * S.N,
+                                     sizeof(double) * S.N, S.m, cudaMemcpyDeviceToHost, s));
+    HODLR_CUDA_TRY(cudaStreamSynchronize(s));
+    return rc;
   });
 }
 

@@ -645,10 +645,15 @@ void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t 
   }
 }
 
+// parts: kPathLeaves (the leaf solves / factorization), kPathLevels (the
+// tree levels), or both; the levels read nothing of V before their first
+// reduce, so a caller can let V arrive in between
 template <typename T, typename TE>
-void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cudaStream_t s) {
+void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cudaStream_t s,
+              int parts = kPathLeaves | kPathLevels) {
   LeafTask<T> none{};
-  if (plan.factor) {
+  if (!(parts & kPathLeaves)) {
+  } else if (plan.factor) {
     run_leaf_plan<T>(pf, plan.leaf, info, s);
   } else if (plan.apply_nb > 0) {
     PhaseScope ps(pf, PH_GETRS, s);
@@ -658,6 +663,7 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
     PhaseScope ps(pf, PH_GETRS, s);
     launch_getrs<T>(plan.leaf_tasks.p, none, plan.nleaf, plan.max_n, plan.max_nrhs, s);
   }
+  if (!(parts & kPathLevels)) return;
   if (!plan.factor && plan.sweep_ok && sweep_persistent_enabled()) {
     PhaseScope ps(pf, PH_SWEEP_LEVELS, s);
     launch_sweep_levels(plan.sweep.p, (int)plan.levels.size(), plan.sweep_max_n,
@@ -1151,23 +1157,30 @@ void System::run_apply64(cudaStream_t s) {
 }
 
 void System::run_factor32(cudaStream_t s) {
-  convert32(s);
-  run_path(prof, fused32, 0, info.p, s);
-  factored = HODLR_PREC_MIXED;
-  factored_form = 0;
+  run_factor32_part(kPathLeaves | kPathLevels, s);
 }
 
-void System::convert32(cudaStream_t s) {
+void System::run_factor32_part(int parts, cudaStream_t s) {
+  convert32(parts, s);
+  run_path(prof, fused32, 0, info.p, s, parts);
+  if (parts & kPathLevels) {
+    factored = HODLR_PREC_MIXED;
+    factored_form = 0;
+  }
+}
+
+void System::convert32(int parts, cudaStream_t s) {
   ensure_mixed();
   const long long n = N;
   {
     PhaseScope ps(prof, PH_CONVERT, s);
-    launch_convert2d<double, float>(D.p, n, D32.p, n, n, nmax, s);
-    launch_convert2d<double, float>(B.p, n, X32.p, n, n, m, s);
-    if (vc > 0) {
-      launch_convert2d<double, float>(U.p, n, X32.p + (size_t)n * m, n, n, vc, s);
-      launch_convert2d<double, float>(V.p, n, V32.p, n, n, vc, s);
+    if (parts & kPathLeaves) {  // what the leaf factorization reads: D and [b | U]
+      launch_convert2d<double, float>(D.p, n, D32.p, n, n, nmax, s);
+      launch_convert2d<double, float>(B.p, n, X32.p, n, n, m, s);
+      if (vc > 0) launch_convert2d<double, float>(U.p, n, X32.p + (size_t)n * m, n, n, vc, s);
     }
+    if ((parts & kPathLevels) && vc > 0)  // V, first read by the levels' reduce
+      launch_convert2d<double, float>(V.p, n, V32.p, n, n, vc, s);
   }
 }
 

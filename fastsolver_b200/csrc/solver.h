@@ -233,6 +233,30 @@ void run_graph(GraphSeg &g, bool eager, cudaStream_t s, F &&fn) {
   add_launches(g.kernels);
 }
 
+// part masks of a path: the leaf solves / factorization and the tree levels
+constexpr int kPathLeaves = 1, kPathLevels = 2;
+
+// A stream for copies of host input and two events on it, created on first
+// use (hodlr_solve_refined_host)
+struct CopyLane {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t inputs = nullptr;  // D, B and U copied (recorded on the solve stream)
+  cudaEvent_t v = nullptr;       // V copied (recorded on the copy stream)
+  CopyLane() = default;
+  CopyLane(const CopyLane &) = delete;
+  CopyLane &operator=(const CopyLane &) = delete;
+  ~CopyLane() {
+    if (inputs) cudaEventDestroy(inputs);
+    if (v) cudaEventDestroy(v);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void ensure() {
+    if (!stream) HODLR_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    if (!inputs) HODLR_CUDA_TRY(cudaEventCreateWithFlags(&inputs, cudaEventDisableTiming));
+    if (!v) HODLR_CUDA_TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
+  }
+};
+
 struct System {
   Tree tree;
   int N = 0, m = 0, r = 0, C = 0, vc = 0, nmax = 0;
@@ -267,6 +291,8 @@ struct System {
   Profiler prof;
   bool use_graphs = true;  // replay captured segments (off while profiling)
   GraphSeg g_factor32, g_sweep32, g_factor64, g_fused64[2], g_sweep64;
+  GraphSeg g_factor32_leaves, g_factor32_levels;  // run_factor32 in two parts
+  CopyLane lane;  // copies of host input (hodlr_solve_refined_host)
 
   int init(int N_, int nrhs, int rank, int threshold);
   void ensure_fp64();
@@ -275,7 +301,10 @@ struct System {
   void run_fused64(int form, cudaStream_t s);     // X64 = [B|U], DLU64 = D, walk
   void run_apply64(cudaStream_t s);               // Y64 <- A^{-1} Y64 with fused64 factors
   void run_factor32(cudaStream_t s);              // X32 = f32([B|U]), D32 = f32(D), walk
-  void convert32(cudaStream_t s);                 // the FP64 -> FP32 copies of run_factor32
+  // one part of run_factor32 (kPathLeaves: conversion of D, [B|U] and the
+  // leaf factorization; kPathLevels: conversion of V and the tree levels)
+  void run_factor32_part(int parts, cudaStream_t s);
+  void convert32(int parts, cudaStream_t s);      // the FP64 -> FP32 copies of those parts
   void run_apply32(cudaStream_t s);               // Y32 <- A^{-1} Y32
   void run_matvec(const MatvecPlan &p, double alpha, double beta, cudaStream_t s);
   int check_info(cudaStream_t s);                 // sync + first nonzero INFO
@@ -288,6 +317,7 @@ struct System {
   }
   void reset_graphs() {
     g_factor32.reset(); g_sweep32.reset(); g_factor64.reset(); g_sweep64.reset();
+    g_factor32_leaves.reset(); g_factor32_levels.reset();
     g_fused64[0].reset(); g_fused64[1].reset();
   }
 };

@@ -297,6 +297,28 @@ class FastSolver:
             check("hodlr_solve_refined", st)
         return it.value, rr.value
 
+    def solve_refined_host(self, matrix: HodlrMatrix, D, U, V, B, out=None,
+                           precision: int = PREC_MIXED, tol: float = 1e-12, maxiter: int = 10,
+                           stream=None, check_conv=True):
+        """Host-to-host refined solve: D, U, V, B are column-major host arrays
+        (numpy, or pinned CPU torch tensors for overlapped copies), `out` an
+        optional column-major host array (N x nrhs) for the solution.  Returns
+        (x, sweeps, relres)."""
+        ins = [x if hasattr(x, "data_ptr") else _fortran(x) for x in (D, U, V, B)]
+        if out is None:
+            out = np.zeros((matrix.rhs_rows, matrix.rhs_cols), dtype=np.float64, order="F")
+        it = ctypes.c_int()
+        rr = ctypes.c_double()
+        args = []
+        for x in ins:
+            args += [_ptr(x), _ld(x)]
+        st = lib.hodlr_solve_refined_host(matrix.handle, *args, _ptr(out), _ld(out),
+                                          int(precision), float(tol), int(maxiter),
+                                          ctypes.byref(it), ctypes.byref(rr), _stream_ptr(stream))
+        if check_conv or st != _lib.ERR_NOCONV:
+            check("hodlr_solve_refined_host", st)
+        return out, it.value, rr.value
+
 
 def _tune(fn, name, tol, reps, cap=64):
     best = _lib.Schedule()

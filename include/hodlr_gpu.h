@@ -244,6 +244,22 @@ int hodlr_solve_refined(hodlr_system sys, int precision, double tol,
                         int maxiter, int *iters, double *relres,
                         hodlr_stream_t stream);
 
+/* The same refined solve from host memory to host memory: copies D, U, V
+ * and B in (as hodlr_set_matrix / hodlr_set_rhs with host = 1), solves, and
+ * copies the solution out to X (N x nrhs, ldx), all on `stream`; returns
+ * when X holds the result and no copy still reads the caller's buffers.
+ * With PREC_MIXED, V's copy (first read by the tree levels) runs on a
+ * second stream under the leaf factorization; from pinned host memory the
+ * copy and the factorization overlap.  U and V may be NULL only for a
+ * system without off-diagonal blocks.  Return values as
+ * hodlr_solve_refined; negative: the position of an invalid argument. */
+int hodlr_solve_refined_host(hodlr_system sys, const double *D, long long ldd,
+                             const double *U, long long ldu, const double *V,
+                             long long ldv, const double *B, long long ldb,
+                             double *X, long long ldx, int precision, double tol,
+                             int maxiter, int *iters, double *relres,
+                             hodlr_stream_t stream);
+
 /* y = A x (FP64 HODLR matvec) for x, y device arrays N x ncols (ldx, ldy),
  * ncols <= nrhs. */
 int hodlr_matvec(hodlr_system sys, const double *x, long long ldx, double *y,

@@ -69,6 +69,8 @@ def test_argument_errors_are_reported_before_device_use(fs):
     assert lib.hodlr_set_schedule(None, None) == -1
     assert lib.hodlr_autotune(None, 1, 1e-12, 2, None, None, None, 0, None) == -1
     assert lib.hodlr_batch_autotune(None, 1e-12, 2, None, None, None, 0, None) == -1
+    assert lib.hodlr_solve_refined_host(None, None, 0, None, 0, None, 0, None, 0, None, 0, 1,
+                                        1e-12, 10, None, None, None) == -1
 
 
 def test_schedule_cache_key(fs):

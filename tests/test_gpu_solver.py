@@ -197,3 +197,37 @@ def test_graph_replay_new_rhs(fs, oracle, cuda, precision):
         st.synchronize()
         Xo, _ = oracle.bfs_solve(s, nthreads=8)
         assert relerr(h.solution(stream=st), Xo[:, :m]) < 1e-12
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_solve_refined_host_matches_device_path(fs, oracle, cuda, precision):
+    """The host-to-host refined solve (inputs copied in, V's copy under the
+    leaf factorization for the mixed path, the solution copied out) gives
+    bit for bit the solution of the device-resident solve, from pinned
+    tensors on a side stream and from pageable arrays on the legacy stream,
+    and repeated calls replay it unchanged."""
+    import torch
+    N, m, r, t = 20000, 4, 40, 512
+    s = make_gauss(oracle, N, m, r, t, seed=31)
+    prec = fs.PREC_MIXED if precision == "mixed" else fs.PREC_FP64
+    h = gpu_system(fs, s)
+    it1, rr1 = fs.FastSolver().solve_refined(h, prec, tol=1e-12, maxiter=10)
+    x1 = h.solution()
+    assert rr1 <= 1e-12
+
+    def pinned(a):  # column-major pinned CPU tensor
+        return torch.from_numpy(np.ascontiguousarray(np.asfortranarray(a).T)).pin_memory().t()
+
+    h2 = fs.HodlrMatrix(m, N, r, t).create_tree()
+    st = torch.cuda.Stream()
+    sol = fs.FastSolver()
+    x2, it2, rr2 = sol.solve_refined_host(h2, pinned(s.D), pinned(s.U), pinned(s.V), pinned(s.B),
+                                          precision=prec, stream=st)
+    assert it2 == it1 and rr2 == rr1
+    np.testing.assert_array_equal(x2, x1)
+    for _ in range(2):
+        x3, it3, _ = sol.solve_refined_host(h2, s.D, s.U, s.V, s.B, precision=prec)
+        assert it3 == it1
+        np.testing.assert_array_equal(x3, x1)
+    Xo, _ = oracle.bfs_solve(s, nthreads=8)
+    assert relerr(x1, Xo[:, :m]) < 1e-11
