@@ -845,24 +845,28 @@ int hodlr_solve(hodlr_system h, hodlr_stream_t stream) {
 }
 
 // The refined solve of one system on stream s (see hodlr_solve_refined).
-// With v_ready, the mixed factor pass runs as two segments, the leaf
-// factorization and the tree levels, and s waits for v_ready (V on the
-// device) between them.
+// With `lane` (V still being copied in on lane->stream, lane->level_v[l]
+// recorded once level l's columns of V are in, lane->v once all are), the
+// mixed factor pass replays its leaf factorization, then runs the levels
+// eagerly, each after its own columns of V arrived (converted to FP32 just
+// before it), and the residual after all of V.
 static int refined_body(System &S, int precision, double tol, int maxiter, int *iters,
-                        double *relres, cudaStream_t s, cudaEvent_t v_ready = nullptr) {
+                        double *relres, cudaStream_t s, const CopyLane *lane = nullptr) {
   const long long N = S.N;
   const size_t nm = (size_t)N * S.m;
   // two replayable segments: factor pass + residual, and one refinement
   // sweep + residual (captured as CUDA graphs on the first call)
-  if (precision == HODLR_PREC_MIXED && v_ready) {
+  if (precision == HODLR_PREC_MIXED && lane) {
     S.ensure_mixed();
     S.run_graph(S.g_factor32_leaves, s, [&]() { S.run_factor32_part(kPathLeaves, s); });
-    HODLR_CUDA_TRY(cudaStreamWaitEvent(s, v_ready, 0));
-    S.run_graph(S.g_factor32_levels, s, [&]() {
-      S.run_factor32_part(kPathLevels, s);
-      launch_convert2d<float, double>(S.X32.p, N, S.Xsol.p, N, N, S.m, s);
-      S.relres_enqueue(s);
-    });
+    const LevelHook hook = [&](int l, int lo, int hi) {
+      HODLR_CUDA_TRY(cudaStreamWaitEvent(s, lane->level_v[l], 0));
+      S.convert_v32(lo, hi, s);
+    };
+    S.run_factor32_levels_hooked(hook, s);
+    HODLR_CUDA_TRY(cudaStreamWaitEvent(s, lane->v, 0));  // the residual reads all of V
+    launch_convert2d<float, double>(S.X32.p, N, S.Xsol.p, N, N, S.m, s);
+    S.relres_enqueue(s);
     S.factored = HODLR_PREC_MIXED;
     S.factored_form = 0;
   } else if (precision == HODLR_PREC_MIXED) {
@@ -958,21 +962,36 @@ int hodlr_solve_refined_host(hodlr_system h, const double *D, long long ldd, con
     copy2d(S.B.p, S.N, B, ldb, S.N, S.m, 1, s);
     if (S.vc > 0) copy2d(S.U.p, S.N, U, ldu, S.N, S.vc, 1, s);
     S.factored = -1;
-    cudaEvent_t v_ready = nullptr;
+    const CopyLane *lane = nullptr;
     if (S.vc > 0 && precision == HODLR_PREC_MIXED) {
-      // V is first read by the tree levels: its copy follows the others on
-      // the copy lane, under the leaf factorization
+      // V is first read by the tree levels, each level only its children's
+      // columns: V follows the other copies on the copy lane, in the levels'
+      // order (deepest first), one event per level, under the leaf
+      // factorization and the levels before
+      S.ensure_mixed();
+      const auto &lv = S.fused32.levels;
       S.lane.ensure();
+      S.lane.ensure_levels(lv.size());
       drain.st = S.lane.stream;
       HODLR_CUDA_TRY(cudaEventRecord(S.lane.inputs, s));
       HODLR_CUDA_TRY(cudaStreamWaitEvent(S.lane.stream, S.lane.inputs, 0));
-      copy2d(S.V.p, S.N, V, ldv, S.N, S.vc, 1, S.lane.stream);
+      int covered = S.vc;  // columns [covered, vc) of V are on their way
+      for (size_t l = 0; l < lv.size(); ++l) {
+        const int lo = lv[l]->v_hi > lv[l]->v_lo ? std::min(lv[l]->v_lo, covered) : covered;
+        if (lo < covered) {
+          copy2d(S.V.p + (size_t)lo * S.N, S.N, V + (size_t)lo * ldv, ldv, S.N, covered - lo, 1,
+                 S.lane.stream);
+          covered = lo;
+        }
+        HODLR_CUDA_TRY(cudaEventRecord(S.lane.level_v[l], S.lane.stream));
+      }
+      if (covered > 0) copy2d(S.V.p, S.N, V, ldv, S.N, covered, 1, S.lane.stream);
       HODLR_CUDA_TRY(cudaEventRecord(S.lane.v, S.lane.stream));
-      v_ready = S.lane.v;
+      lane = &S.lane;
     } else if (S.vc > 0) {
       copy2d(S.V.p, S.N, V, ldv, S.N, S.vc, 1, s);
     }
-    const int rc = refined_body(S, precision, tol, maxiter, iters, relres, s, v_ready);
+    const int rc = refined_body(S, precision, tol, maxiter, iters, relres, s, lane);
     HODLR_CUDA_TRY(cudaMemcpy2DAsync(X, sizeof(double) * ldx, S.Xsol.p, sizeof(double) * S.N,
                                      sizeof(double) * S.N, S.m, cudaMemcpyDeviceToHost, s));
     HODLR_CUDA_TRY(cudaStreamSynchronize(s));

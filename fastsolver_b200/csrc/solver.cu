@@ -405,10 +405,15 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
     std::vector<GemmItem<T, T>> ai;
     std::vector<GemmSeg<T>> as;
     size_t poff = 0, woff = 0, eoff = 0;
+    L->v_lo = 1 << 30;
     for (int p : ids) {
       const Node &P = t.nodes[p];
       const Node &c0 = t.nodes[P.lchild], &c1 = t.nodes[P.rchild];
       const int cw = sp.factor ? c0.col_beg : m;
+      for (const Node *c : {&c0, &c1}) {
+        L->v_lo = std::min(L->v_lo, c->col_beg - m);
+        L->v_hi = std::max(L->v_hi, c->col_beg - m + c->vncol);
+      }
       NodeTask<T, TE> k{};
       const T *W0d = nullptr, *W1d = nullptr;
       long long ldw0d = 0, ldw1d = 0;
@@ -650,7 +655,7 @@ void run_leaf_plan(Profiler &pf, const LeafPlan<T> &lp, int *info, cudaStream_t 
 // reduce, so a caller can let V arrive in between
 template <typename T, typename TE>
 void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cudaStream_t s,
-              int parts = kPathLeaves | kPathLevels) {
+              int parts = kPathLeaves | kPathLevels, const LevelHook *hook = nullptr) {
   LeafTask<T> none{};
   if (!(parts & kPathLeaves)) {
   } else if (plan.factor) {
@@ -670,8 +675,11 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
                         plan.sweep_bar.p, s);
     return;
   }
+  int li = 0;
   for (const auto &Lp : plan.levels) {
     const LevelPlan<T, TE> &L = *Lp;
+    if (hook) (*hook)(li, L.v_lo, L.v_hi);
+    ++li;
     {
       PhaseScope ps(pf, PH_REDUCE, s);
       launch_gemm_items<T, T, T>(L.red_items.p, L.red_segs.p, L.n_red, L.red_max_m,
@@ -1167,6 +1175,19 @@ void System::run_factor32_part(int parts, cudaStream_t s) {
     factored = HODLR_PREC_MIXED;
     factored_form = 0;
   }
+}
+
+void System::run_factor32_levels_hooked(const LevelHook &hook, cudaStream_t s) {
+  ensure_mixed();
+  run_path(prof, fused32, 0, info.p, s, kPathLevels, &hook);
+  factored = HODLR_PREC_MIXED;
+  factored_form = 0;
+}
+
+void System::convert_v32(int lo, int hi, cudaStream_t s) {
+  if (hi <= lo) return;
+  PhaseScope ps(prof, PH_CONVERT, s);
+  launch_convert2d<double, float>(V.p + (size_t)lo * N, N, V32.p + (size_t)lo * N, N, N, hi - lo, s);
 }
 
 void System::convert32(int parts, cudaStream_t s) {

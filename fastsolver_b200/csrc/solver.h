@@ -3,6 +3,7 @@
 // src/solver/fast_solver.cc:56-72, 136-255).
 #pragma once
 
+#include <functional>
 #include <memory>
 #include <vector>
 
@@ -63,6 +64,7 @@ struct LevelPlan {
   DevBuf<GemmItem<T, T>> red_items;
   DevBuf<GemmSeg<T>> red_segs;
   int n_red = 0, red_max_m = 0, red_max_n = 0;
+  int v_lo = 0, v_hi = 0;  // columns of V its reduce reads: [v_lo, v_hi)
   DevBuf<SumTask<T>> sums;          // partial slots -> one W per child
   int n_sums = 0;
   long long sum_max_len = 0;
@@ -235,6 +237,9 @@ void run_graph(GraphSeg &g, bool eager, cudaStream_t s, F &&fn) {
 
 // part masks of a path: the leaf solves / factorization and the tree levels
 constexpr int kPathLeaves = 1, kPathLevels = 2;
+// called before each level of a path, in order: (level index, the columns of
+// V its reduce reads [v_lo, v_hi))
+using LevelHook = std::function<void(int, int, int)>;
 
 // A stream for copies of host input and two events on it, created on first
 // use (hodlr_solve_refined_host)
@@ -242,10 +247,12 @@ struct CopyLane {
   cudaStream_t stream = nullptr;
   cudaEvent_t inputs = nullptr;  // D, B and U copied (recorded on the solve stream)
   cudaEvent_t v = nullptr;       // V copied (recorded on the copy stream)
+  std::vector<cudaEvent_t> level_v;  // V's columns of level l copied
   CopyLane() = default;
   CopyLane(const CopyLane &) = delete;
   CopyLane &operator=(const CopyLane &) = delete;
   ~CopyLane() {
+    for (cudaEvent_t e : level_v) cudaEventDestroy(e);
     if (inputs) cudaEventDestroy(inputs);
     if (v) cudaEventDestroy(v);
     if (stream) cudaStreamDestroy(stream);
@@ -254,6 +261,13 @@ struct CopyLane {
     if (!stream) HODLR_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     if (!inputs) HODLR_CUDA_TRY(cudaEventCreateWithFlags(&inputs, cudaEventDisableTiming));
     if (!v) HODLR_CUDA_TRY(cudaEventCreateWithFlags(&v, cudaEventDisableTiming));
+  }
+  void ensure_levels(size_t n) {
+    while (level_v.size() < n) {
+      cudaEvent_t e = nullptr;
+      HODLR_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      level_v.push_back(e);
+    }
   }
 };
 
@@ -291,7 +305,7 @@ struct System {
   Profiler prof;
   bool use_graphs = true;  // replay captured segments (off while profiling)
   GraphSeg g_factor32, g_sweep32, g_factor64, g_fused64[2], g_sweep64;
-  GraphSeg g_factor32_leaves, g_factor32_levels;  // run_factor32 in two parts
+  GraphSeg g_factor32_leaves;  // the leaf part of run_factor32 (hodlr_solve_refined_host)
   CopyLane lane;  // copies of host input (hodlr_solve_refined_host)
 
   int init(int N_, int nrhs, int rank, int threshold);
@@ -304,7 +318,11 @@ struct System {
   // one part of run_factor32 (kPathLeaves: conversion of D, [B|U] and the
   // leaf factorization; kPathLevels: conversion of V and the tree levels)
   void run_factor32_part(int parts, cudaStream_t s);
+  // the levels part with `hook` before each level, V converted level by level
+  // inside the hook's caller (run_factor32_levels_hooked)
+  void run_factor32_levels_hooked(const LevelHook &hook, cudaStream_t s);
   void convert32(int parts, cudaStream_t s);      // the FP64 -> FP32 copies of those parts
+  void convert_v32(int lo, int hi, cudaStream_t s);  // V32 = f32(V) for columns [lo, hi)
   void run_apply32(cudaStream_t s);               // Y32 <- A^{-1} Y32
   void run_matvec(const MatvecPlan &p, double alpha, double beta, cudaStream_t s);
   int check_info(cudaStream_t s);                 // sync + first nonzero INFO
@@ -317,7 +335,7 @@ struct System {
   }
   void reset_graphs() {
     g_factor32.reset(); g_sweep32.reset(); g_factor64.reset(); g_sweep64.reset();
-    g_factor32_leaves.reset(); g_factor32_levels.reset();
+    g_factor32_leaves.reset();
     g_fused64[0].reset(); g_fused64[1].reset();
   }
 };
