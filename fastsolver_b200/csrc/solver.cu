@@ -331,6 +331,7 @@ void build_sweep(PathPlan<T, TE> &plan) {
       d.sums = L.sums.p;
       d.n_sums = L.n_sums;
       d.sum_units = (int)cdiv<long long>(std::max<long long>(L.sum_max_len, 1), kSweepSumChunk);
+      d.sum_max_slots = L.sum_max_slots;
       d.ap_items = L.ap_items.p;
       d.ap_segs = L.ap_segs.p;
       d.n_ap = L.n_ap;
@@ -459,6 +460,7 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
           st.nslots = nslots;
           su.push_back(st);
           L->sum_max_len = std::max(L->sum_max_len, st.len);
+          L->sum_max_slots = std::max(L->sum_max_slots, nslots);
         }
         if (side == 0) {
           W0d = W; k.W0u = W + (size_t)M * (NW - c.ncol);
@@ -969,6 +971,7 @@ void merge_paths(const std::vector<const PathPlan<T, TE> *> &src, const std::vec
       bc.add(S.bc_items.h, S.bc_segs.h);
       su.insert(su.end(), S.sums.h.begin(), S.sums.h.end());
       L->sum_max_len = std::max(L->sum_max_len, S.sum_max_len);
+      L->sum_max_slots = std::max(L->sum_max_slots, S.sum_max_slots);
       for (int f = 0; f < 2; ++f) {
         for (NodeTask<T, TE> t : S.node_tasks[f].h) {
           t.info_slot += info_off[k];

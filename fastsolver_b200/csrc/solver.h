@@ -67,6 +67,7 @@ struct LevelPlan {
   int v_lo = 0, v_hi = 0;  // columns of V its reduce reads: [v_lo, v_hi)
   DevBuf<SumTask<T>> sums;          // partial slots -> one W per child
   int n_sums = 0;
+  int sum_max_slots = 0;             // most partial slots of one of its tasks
   long long sum_max_len = 0;
   DevBuf<GemmItem<T, double>> gram_items;  // S = I - V1Tu1 V0Tu0, FP64 result
   DevBuf<GemmSeg<T>> gram_segs;

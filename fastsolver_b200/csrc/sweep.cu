@@ -42,6 +42,7 @@ namespace {
 using namespace sk;
 constexpr int kThreads = 128;
 constexpr long long kSweepSpinDefault = 1LL << 22;
+constexpr int kSweepWarpSlots = 32;  // slot counts summed by one warp per unit
 
 // Grid barrier; false when the kernel is being abandoned (a wait ran out).
 // bar[0] counts arrivals; the CTA whose arrival completes barrier k publishes
@@ -115,24 +116,43 @@ __global__ void __launch_bounds__(kThreads, 3)
     }
     if (!grid_sync(bar, gen, limit)) return;
     // slot sums in a fixed order (the REDOP_ADD of gemm.cc:74-133,
-    // deterministic): a unit is 32 elements of one task; warp w adds slots
-    // w, w + 4, ..., then warp 0 adds the four partial sums in order
+    // deterministic); a unit is 32 elements of one task.  Levels whose tasks
+    // have at most kSweepWarpSlots slots (the deepest ones: thousands of
+    // small tasks): every warp takes a unit of its own and adds its slots in
+    // order, with no barrier.  Otherwise warp w of the CTA adds slots w,
+    // w + 4, ... of a unit, then warp 0 adds the four partial sums in order.
     {
-      double *part = reinterpret_cast<double *>(smem);  // [4][32]
       const int lane = tid & 31, w = tid >> 5;
       const int nu = L.n_sums * L.sum_units;
-      for (int u = blockIdx.x; u < nu; u += gridDim.x) {
-        const SumTask<float> tk = L.sums[u / L.sum_units];
-        const long long e = (long long)(u % L.sum_units) * kSweepSumChunk + lane;
-        double acc = 0.0;
-        if (e < tk.len)
-          for (int q = w; q < tk.nslots; q += kThreads / 32)
-            acc += double(__ldcg(tk.src + e + (long long)q * tk.stride));
-        part[w * 32 + lane] = acc;
-        __syncthreads();
-        if (w == 0 && e < tk.len)
-          tk.dst[e] = float(((part[lane] + part[32 + lane]) + part[64 + lane]) + part[96 + lane]);
-        __syncthreads();
+      if (L.sum_max_slots <= kSweepWarpSlots) {
+        constexpr int kWarps = kThreads / 32;
+        for (int u = blockIdx.x * kWarps + w; u < nu; u += gridDim.x * kWarps) {
+          const SumTask<float> tk = L.sums[u / L.sum_units];
+          const long long e = (long long)(u % L.sum_units) * kSweepSumChunk + lane;
+          if (e < tk.len) {
+            double acc = 0.0;
+#pragma unroll 4
+            for (int q = 0; q < tk.nslots; ++q) acc += double(__ldcg(tk.src + e + (long long)q * tk.stride));
+            tk.dst[e] = float(acc);
+          }
+        }
+      } else {
+        double *part = reinterpret_cast<double *>(smem);  // [4][32]
+        for (int u = blockIdx.x; u < nu; u += gridDim.x) {
+          const SumTask<float> tk = L.sums[u / L.sum_units];
+          const long long e = (long long)(u % L.sum_units) * kSweepSumChunk + lane;
+          double acc = 0.0;
+          if (e < tk.len) {
+#pragma unroll 8
+            for (int q = w; q < tk.nslots; q += kThreads / 32)
+              acc += double(__ldcg(tk.src + e + (long long)q * tk.stride));
+          }
+          part[w * 32 + lane] = acc;
+          __syncthreads();
+          if (w == 0 && e < tk.len)
+            tk.dst[e] = float(((part[lane] + part[32 + lane]) + part[64 + lane]) + part[96 + lane]);
+          __syncthreads();
+        }
       }
     }
     if (!grid_sync(bar, gen, limit)) return;

@@ -18,6 +18,7 @@ struct SweepLevel {
   const GemmSeg<float> *bc_segs;
   int n_red, red_mt, red_nt;  // items, 64-row and 16-column blocks per item
   int n_sums, sum_units;      // tasks, kSweepSumChunk-element chunks per task
+  int sum_max_slots;          // most partial slots of one task
   int n_ap, ap_rb;            // items, 128-row blocks per item
   int n_bc, bc_rb;
 };
