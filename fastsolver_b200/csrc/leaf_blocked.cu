@@ -391,9 +391,28 @@ __global__ void __launch_bounds__(kRegThreads, 1)
                   if (cv * VW >= QW && (cv * VW) / QW >= live_blocks) continue;
                   const V v = prow[cv];
                   const T *vp = reinterpret_cast<const T *>(&v);
+                  if constexpr (sizeof(T) == 4) {
+                    // pairs of columns through the packed FP32 FMA (each
+                    // half rounded as the scalar a - l p); which columns
+                    // change is known at compile time (jj is unrolled)
+                    const float2 nl = make_float2(-float(l), -float(l));
 #pragma unroll
-                  for (int u = 0; u < VW; ++u)
-                    if (cv * VW + u > jj) a[q][cv * VW + u] -= l * vp[u];
+                    for (int u = 0; u < VW; u += 2) {
+                      const int c = cv * VW + u;
+                      if (c > jj) {
+                        const float2 r = __ffma2_rn(nl, make_float2(vp[u], vp[u + 1]),
+                                                    make_float2(a[q][c], a[q][c + 1]));
+                        a[q][c] = r.x;
+                        a[q][c + 1] = r.y;
+                      } else if (c + 1 > jj) {
+                        a[q][c + 1] -= l * vp[u + 1];
+                      }
+                    }
+                  } else {
+#pragma unroll
+                    for (int u = 0; u < VW; ++u)
+                      if (cv * VW + u > jj) a[q][cv * VW + u] -= l * vp[u];
+                  }
                 }
               }
             }
