@@ -679,7 +679,10 @@ def main():
     per_launch_ms = ms_upd / max(n_upd, 1)
     bytes_per_launch = upd_bytes / max(n_upd, 1)
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
-    traffic = profile_traffic(os.path.join(ROOT, "profiles", "leaf_update_gemm_n262144.md"))
+    # DRAM bytes per launch from the ncu capture of this workload (recorded
+    # for the 262144-row system only; none for the other configs)
+    traffic = (profile_traffic(os.path.join(ROOT, "profiles", "leaf_update_gemm_n262144.md"))
+               if args.config == "n262144" else None)
     roofline = {"bound": "hbm", "kernel": "tc_gemm_persistent<128,false,float,true> (leaf trailing update)",
                 "achieved": achieved, "peak": pk["hbm"], "unit": "GB/s",
                 "frac": achieved / pk["hbm"], "traffic": traffic,
