@@ -21,7 +21,8 @@
 // node -- one CTA per node, S^{-1} by Gauss-Jordan elimination with partial
 // pivoting (pivot = largest |a|, lowest row on ties, as LAPACK's idamax; in
 // registers for s <= 64, in shared memory above), the three products from
-// shared memory and L2 -- and the
+// shared memory and L2 (and S itself where V0Tu0, V1Tu1 fit in shared
+// memory) -- and the
 // solver applies M to every column block as one batched GEMM per level (the
 // same engine as the reduce and broadcast), for the fused pass and for every
 // later solve with the same factors.  INFO > 0 reports an exactly zero pivot
@@ -266,7 +267,13 @@ __global__ void __launch_bounds__(kNodeThreads)
       W1s[e] = double(tk.W1u[i + (long long)j * tk.ldw1u]);
     }
   }
-  if (form == 0) {
+  if (form == 0 && stage) {
+    // S = I - V1Tu1 V0Tu0 (the dgemm at solver_tasks.cc:261) from the staged
+    // FP64 copies, on the DMMA pipe, straight into the elimination's matrix
+    __syncthreads();
+    node_product_dmma(r0, r0, r1, -1.0, true, W1s, r0, W0s, r1,
+                      [&](int i, int c, double v) { A[i * lda + c] = v; });
+  } else if (form == 0) {
     for (int e = tid; e < s * s; e += kNodeThreads) {
       const int i = e % s, c = e / s;
       A[i * lda + c] = tk.S[e];
@@ -466,14 +473,17 @@ __global__ void __launch_bounds__(kNodeThreads)
 
 size_t node_factor_smem(int max_s) { return node_factor_words(max_s) * sizeof(double); }
 
+bool node_factor_stages(int max_s, int max_r) {
+  return node_factor_smem(max_s) + 4 * (size_t)max_r * max_r * sizeof(double) <= 200 * 1024;
+}
+
 template <typename TW, typename TE>
 void launch_node_factor(const NodeTask<TW, TE> *tasks, int count, int max_s, int max_r, int form,
                         int *info, cudaStream_t s) {
   if (count <= 0) return;
   size_t smem = node_factor_smem(max_s);
-  const size_t staged = smem + 4 * (size_t)max_r * max_r * sizeof(double);
-  const int stage = (form == 0 && staged <= 200 * 1024) ? 1 : 0;
-  if (stage) smem = staged;
+  const int stage = (form == 0 && node_factor_stages(max_s, max_r)) ? 1 : 0;
+  if (stage) smem += 4 * (size_t)max_r * max_r * sizeof(double);
   auto go = [&](auto kern) {
     raise_smem_limit(reinterpret_cast<const void *>(kern), smem);
     kern<<<count, kNodeThreads, smem, s>>>(tasks, form, max_s, max_r, stage, info);

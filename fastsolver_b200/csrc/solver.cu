@@ -690,7 +690,9 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
     }
     if (plan.factor) {
       PhaseScope ps(pf, PH_NODE_FACTOR, s);
-      if (L.n_gram > 0)
+      // S = I - V1Tu1 V0Tu0 for the form-0 nodes, unless the node kernel stages
+      // its inputs and forms S itself
+      if (L.n_gram > 0 && !(L.n_nodes[0] > 0 && node_factor_stages(L.max_s[0], L.max_r[0])))
         launch_gemm_items<T, double, double>(L.gram_items.p, L.gram_segs.p, L.n_gram, L.gram_max,
                                              L.gram_max, false, -1.0, 1.0, s);
       for (int f = 0; f < 2; ++f)
