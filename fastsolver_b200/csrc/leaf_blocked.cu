@@ -802,9 +802,21 @@ __device__ inline void tile_mm(const T *A, int lda, const T *B, int ldb, T *C, i
 #pragma unroll
     for (int q = 0; q < R; ++q) b[q] = B[k + (tx * R + q) * ldb];
 #pragma unroll
-    for (int r = 0; r < R; ++r)
+    for (int r = 0; r < R; ++r) {
+      if constexpr (sizeof(T) == 4 && R % 2 == 0) {
+        // packed two-wide FMAs, each half rounded as c + a b
 #pragma unroll
-      for (int q = 0; q < R; ++q) c[r][q] += a[r] * b[q];
+        for (int q = 0; q < R; q += 2) {
+          const float2 v = __ffma2_rn(make_float2(a[r], a[r]), make_float2(b[q], b[q + 1]),
+                                      make_float2(c[r][q], c[r][q + 1]));
+          c[r][q] = v.x;
+          c[r][q + 1] = v.y;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < R; ++q) c[r][q] += a[r] * b[q];
+      }
+    }
   }
 #pragma unroll
   for (int r = 0; r < R; ++r)
