@@ -27,6 +27,8 @@
 // same engine as the reduce and broadcast), for the fused pass and for every
 // later solve with the same factors.  INFO > 0 reports an exactly zero pivot
 // (singular S), as dgesv.
+#include <algorithm>
+
 #include "common.cuh"
 #include "node.cuh"
 
@@ -36,6 +38,8 @@ namespace {
 
 constexpr int kNodeThreads = 512;
 constexpr int kNodeWarps = kNodeThreads / 32;
+// published candidate rows of the register elimination: [2][kNodeWarps][64]
+constexpr size_t kGjScratchWords = 2 * kNodeWarps * 64;
 
 }  // namespace
 
@@ -106,11 +110,12 @@ __device__ inline void node_product(int rows, int cols, int K, double alpha, boo
 // tiles in turn.  Fragments (g = lane / 4, t = lane % 4): A a0 = A[g][t],
 // a1 = A[g + 8][t]; B b = B[t][g]; C c0..c3 = C[g][2t], C[g][2t + 1],
 // C[g + 8][2t], C[g + 8][2t + 1].  Against the SIMT product it reads a
-// fifth of the shared-memory bytes per multiply-add.
-template <typename FO>
+// fifth of the shared-memory bytes per multiply-add.  FP32 operands (the
+// mixed path's staged V^T u blocks) convert to FP64 exactly at the load.
+template <typename TA, typename TB, typename FO>
 __device__ inline void node_product_dmma(int rows, int cols, int K, double alpha,
-                                         bool add_identity, const double *A, int lda,
-                                         const double *B, int ldb, FO out) {
+                                         bool add_identity, const TA *A, int lda, const TB *B,
+                                         int ldb, FO out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int tm = (rows + 15) / 16, tn = (cols + 7) / 8;
@@ -121,9 +126,9 @@ __device__ inline void node_product_dmma(int rows, int cols, int K, double alpha
     for (int k = 0; k < K; k += 4) {
       const int kk = k + t;
       const bool kin = kk < K;
-      const double a0 = (kin && ra < rows) ? A[ra + kk * lda] : 0.0;
-      const double a1 = (kin && rb < rows) ? A[rb + kk * lda] : 0.0;
-      const double b = (kin && cb < cols) ? B[kk + cb * ldb] : 0.0;
+      const double a0 = (kin && ra < rows) ? double(A[ra + kk * lda]) : 0.0;
+      const double a1 = (kin && rb < rows) ? double(A[rb + kk * lda]) : 0.0;
+      const double b = (kin && cb < cols) ? double(B[kk + cb * ldb]) : 0.0;
       asm volatile(
           "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, "
           "{%0, %1, %2, %3};\n"
@@ -153,10 +158,13 @@ __device__ inline void node_product_dmma(int rows, int cols, int K, double alpha
 // matrix in shared memory.  On return A holds the eliminated matrix (the
 // input of the inverse's gather), piv[k] the interchange of step k, at[i] the
 // storage row at final position i, *s_info the first zero pivot (1-based) or
-// 0.  Every thread of the CTA calls it.
-__device__ inline void gj_registers(double *A, int lda, int s, int *piv, int *at, int *s_info) {
+// 0.  scratch: kGjScratchWords doubles of shared memory for the published
+// candidate rows (the caller's, so that it can share them with buffers that
+// are dead during the elimination).  Every thread of the CTA calls it.
+__device__ inline void gj_registers(double *A, int lda, int s, int *piv, int *at, int *s_info,
+                                    double *scratch) {
   constexpr int NWG = kNodeWarps;
-  __shared__ __align__(16) double wrow[2][NWG][64];
+  auto wrow = reinterpret_cast<double (*)[NWG][64]>(scratch);  // [2][NWG][64]
   __shared__ double wval[2][NWG];
   __shared__ int wpos[2][NWG], wcode[2][NWG];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -237,7 +245,7 @@ __device__ inline void gj_registers(double *A, int lda, int s, int *piv, int *at
 template <typename TW, typename TE, int RL>
 __global__ void __launch_bounds__(kNodeThreads)
     node_factor_kernel(const NodeTask<TW, TE> *tasks, int form, int max_s, int max_r, int stage,
-                       int *info) {
+                       int galias, int *info) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const NodeTask<TW, TE> tk = tasks[blockIdx.x];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -249,22 +257,29 @@ __global__ void __launch_bounds__(kNodeThreads)
   int *piv = reinterpret_cast<int *>(A + (size_t)s * lda + 2 * s);
   int *src = piv + s;
   int *at = src + s;
-  // form 0 with stage != 0: V0Tu0, V1Tu1 and G0 as FP64 in shared memory
-  double *W0s = reinterpret_cast<double *>(smem_raw) + node_factor_words(max_s);
-  double *W1s = W0s + (size_t)max_r * max_r;
-  double *Gs = W1s + (size_t)max_r * max_r;
-  double *Ss = Gs + (size_t)max_r * max_r;  // S^{-1} un-permuted, column-major (staged form 0)
+  // form 0 with stage != 0: V0Tu0 and V1Tu1 in shared memory in their own
+  // precision (the products convert them), then S^{-1} un-permuted and
+  // G0 = -S^{-1} V1Tu1, both FP64 column-major.  With galias (r1 <= r0 + 1
+  // for every node of the launch) G0 takes the eliminated matrix's place,
+  // which is dead once S^{-1} has been gathered.
+  // The register elimination's candidate-row scratch shares the S^{-1} / G0
+  // region (both are written after the elimination).
+  TW *W0s = reinterpret_cast<TW *>(reinterpret_cast<double *>(smem_raw) + node_factor_words(max_s));
+  TW *W1s = W0s + (stage ? (size_t)max_r * max_r : 0);
+  double *Ts = reinterpret_cast<double *>(W1s + (stage ? (size_t)max_r * max_r : 0));
+  double *Ss = Ts;
+  double *Gs = galias ? A : Ss + (size_t)max_r * max_r;
   __shared__ int s_info;
 
   if (tid == 0) s_info = 0;
   if (form == 0 && stage) {
     for (int e = tid; e < r1 * r0; e += kNodeThreads) {
       const int i = e % r1, j = e / r1;
-      W0s[e] = double(tk.W0u[i + (long long)j * tk.ldw0u]);
+      W0s[e] = tk.W0u[i + (long long)j * tk.ldw0u];
     }
     for (int e = tid; e < r0 * r1; e += kNodeThreads) {
       const int i = e % r0, j = e / r0;
-      W1s[e] = double(tk.W1u[i + (long long)j * tk.ldw1u]);
+      W1s[e] = tk.W1u[i + (long long)j * tk.ldw1u];
     }
   }
   if (form == 0 && stage) {
@@ -290,7 +305,7 @@ __global__ void __launch_bounds__(kNodeThreads)
   __syncthreads();
 
   if constexpr (RL <= 2) {
-    gj_registers(A, lda, s, piv, at, &s_info);
+    gj_registers(A, lda, s, piv, at, &s_info, Ts);
   } else {
     // ---- Gauss-Jordan with implicit row interchanges, one barrier per column.
     // Rows never move; every warp finds the pivot of column k itself (largest
@@ -479,14 +494,25 @@ bool node_factor_stages(int max_s, int max_r) {
 
 template <typename TW, typename TE>
 void launch_node_factor(const NodeTask<TW, TE> *tasks, int count, int max_s, int max_r, int form,
-                        int *info, cudaStream_t s) {
+                        int *info, cudaStream_t s, bool g_alias) {
   if (count <= 0) return;
   size_t smem = node_factor_smem(max_s);
   const int stage = (form == 0 && node_factor_stages(max_s, max_r)) ? 1 : 0;
-  if (stage) smem += 4 * (size_t)max_r * max_r * sizeof(double);
+  const int galias = (stage && g_alias) ? 1 : 0;
+  // staged: V0Tu0, V1Tu1 (TW), then S^{-1} and, unless it reuses A, G0
+  // (FP64); the register elimination's scratch (s <= 64) shares the latter
+  const size_t tail = std::max(
+      stage ? (size_t)max_r * max_r * (galias ? 1 : 2) * sizeof(double) : (size_t)0,
+      max_s <= 64 ? kGjScratchWords * sizeof(double) : (size_t)0);
+  if (stage) smem += (size_t)max_r * max_r * 2 * sizeof(TW);
+  smem += tail;
   auto go = [&](auto kern) {
     raise_smem_limit(reinterpret_cast<const void *>(kern), smem);
-    kern<<<count, kNodeThreads, smem, s>>>(tasks, form, max_s, max_r, stage, info);
+    // the largest shared-memory carveout: two CTAs of up to ~110 KB per SM
+    HODLR_CUDA_TRY(cudaFuncSetAttribute(reinterpret_cast<const void *>(kern),
+                                        cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared));
+    kern<<<count, kNodeThreads, smem, s>>>(tasks, form, max_s, max_r, stage, galias, info);
   };
   if (max_s <= 32) go(node_factor_kernel<TW, TE, 1>);
   else if (max_s <= 64) go(node_factor_kernel<TW, TE, 2>);
@@ -495,8 +521,8 @@ void launch_node_factor(const NodeTask<TW, TE> *tasks, int count, int max_s, int
 }
 
 template void launch_node_factor<double, double>(const NodeTask<double, double> *, int, int,
-                                                 int, int, int *, cudaStream_t);
+                                                 int, int, int *, cudaStream_t, bool);
 template void launch_node_factor<float, float>(const NodeTask<float, float> *, int, int, int,
-                                               int, int *, cudaStream_t);
+                                               int, int *, cudaStream_t, bool);
 
 }  // namespace hodlr

@@ -571,6 +571,7 @@ void build_path(const Tree &t, const PathSpec<T, TE> &sp, PathPlan<T, TE> &plan,
     for (int f = 0; f < 2; ++f) {
       L->node_tasks[f].upload(nt[f]);
       L->n_nodes[f] = (int)nt[f].size();
+      L->g_alias[f] = node_g_alias(nt[f]);
     }
     L->ap_items.upload(ai);
     L->ap_segs.upload(as);
@@ -698,7 +699,7 @@ void run_path(Profiler &pf, const PathPlan<T, TE> &plan, int form, int *info, cu
       for (int f = 0; f < 2; ++f)
         if (L.n_nodes[f] > 0)
           launch_node_factor<T, TE>(L.node_tasks[f].p, L.n_nodes[f], L.max_s[f], L.max_r[f], f,
-                                    info, s);
+                                    info, s, L.g_alias[f]);
     }
     {
       PhaseScope ps(pf, PH_NODE_APPLY, s);
@@ -994,6 +995,7 @@ void merge_paths(const std::vector<const PathPlan<T, TE> *> &src, const std::vec
     for (int f = 0; f < 2; ++f) {
       L->node_tasks[f].upload(nt[f]);
       L->n_nodes[f] = (int)nt[f].size();
+      L->g_alias[f] = node_g_alias(nt[f]);
     }
     dst.levels.push_back(std::move(L));
   }

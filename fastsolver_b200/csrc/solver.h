@@ -76,6 +76,7 @@ struct LevelPlan {
   // permuted Schur system of the nodes inside a Legion leaf)
   DevBuf<NodeTask<T, TE>> node_tasks[2];
   int n_nodes[2] = {0, 0}, max_s[2] = {0, 0}, max_r[2] = {0, 0};
+  bool g_alias[2] = {false, false};  // node_g_alias of each form's tasks
   DevBuf<GemmItem<T, T>> ap_items;  // [eta0; eta1] = M [V0Td0; V1Td1] per node
   DevBuf<GemmSeg<T>> ap_segs;
   int n_ap = 0, ap_max_m = 0, ap_max_n = 0;
