@@ -15,6 +15,8 @@
 //               CTA (128 threads) = 64 x 16 block of C of one item over all
 //               of K; thread = rows (m, m + 32) x 4 columns, the A and B tiles
 //               stored k-contiguous so each thread reads 16-byte vectors along k.
+#include <algorithm>
+
 #include "common.cuh"
 #include "gemm_skinny.cuh"
 #include "skinny_units.cuh"
@@ -33,12 +35,18 @@ constexpr int kSkThreads = 256;
 // per thread, while the matching block of B sits in shared memory.  Small CTAs (128 rows)
 // and no A staging let many CTAs share an SM, which keeps enough loads in
 // flight for the short-K products of the refinement sweeps (K = r).
+// The CTAs (as many as are resident: three per SM at the kernel's 168
+// registers) take the units (item, 128-row block) u = blockIdx.x,
+// blockIdx.x + gridDim.x, ...: at N = 262144 the root's m-column broadcast
+// has 2048 units, which as one CTA each ran in 4.6 waves of short CTAs.
 template <int NC>
 __global__ void __launch_bounds__(kRowThreads)
     skinny_nn_rows_kernel(const GemmItem<float, float> *__restrict__ items,
-                          const GemmSeg<float> *__restrict__ segs, float alpha, float beta) {
+                          const GemmSeg<float> *__restrict__ segs, float alpha, float beta,
+                          int nunits, int rbn) {
   __shared__ __align__(16) float Bs[nn_rows_kc<NC>() * NC];
-  nn_rows_unit<NC>(items, segs, alpha, beta, blockIdx.x, blockIdx.y, Bs);
+  for (int u = blockIdx.x; u < nunits; u += gridDim.x)
+    nn_rows_unit<NC>(items, segs, alpha, beta, u / rbn, u % rbn, Bs);
 }
 
 // ---------------------------------------------------------------- NN
@@ -461,12 +469,23 @@ void launch_skinny(const GemmItem<T, T> *items, const GemmSeg<T> *segs, int nite
     dim3 grid(nitems, cdiv(max_m, TM), cdiv(max_n, TN));
     skinny_tn2_kernel<T><<<grid, kTNThreads, smem, s>>>(items, segs, alpha, beta);
   } else if constexpr (sizeof(T) == 4) {
-    dim3 grid(nitems, cdiv(max_m, kRowThreads));
+    const int rbn = cdiv(max_m, kRowThreads);
+    const long long nunits = (long long)nitems * rbn;
+    if (nunits > 0x7fffffffLL) throw CudaError{cudaErrorInvalidValue};
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    const int grid = (int)std::min<long long>(nunits, 3LL * sms);
+    const int nu = (int)nunits;
     const auto *fi = reinterpret_cast<const GemmItem<float, float> *>(items);
     const auto *fs = reinterpret_cast<const GemmSeg<float> *>(segs);
-    if (max_n <= 8) skinny_nn_rows_kernel<8><<<grid, kRowThreads, 0, s>>>(fi, fs, alpha, beta);
-    else if (max_n <= 16) skinny_nn_rows_kernel<16><<<grid, kRowThreads, 0, s>>>(fi, fs, alpha, beta);
-    else skinny_nn_rows_kernel<32><<<grid, kRowThreads, 0, s>>>(fi, fs, alpha, beta);
+    if (max_n <= 8)
+      skinny_nn_rows_kernel<8><<<grid, kRowThreads, 0, s>>>(fi, fs, alpha, beta, nu, rbn);
+    else if (max_n <= 16)
+      skinny_nn_rows_kernel<16><<<grid, kRowThreads, 0, s>>>(fi, fs, alpha, beta, nu, rbn);
+    else
+      skinny_nn_rows_kernel<32><<<grid, kRowThreads, 0, s>>>(fi, fs, alpha, beta, nu, rbn);
   } else {
     constexpr int KT = nn_kt<T>();
     dim3 grid(nitems, cdiv(max_m, kNNRows));

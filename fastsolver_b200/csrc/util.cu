@@ -193,13 +193,23 @@ __global__ void colratio_batched_kernel(const RatioTask *__restrict__ tasks) {
 }
 
 // dst[t][e] = sum_q src[t] + q * stride, fixed order (deterministic)
+// (the slot values are loaded four at a time ahead of the adds, which keep
+// the order q = 0, 1, 2, ...: the same sums)
 template <typename T>
 __global__ void sum_slots_kernel(const SumTask<T> *__restrict__ tasks) {
   const SumTask<T> tk = tasks[blockIdx.y];
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tk.len;
        e += (long long)gridDim.x * blockDim.x) {
     double acc = 0.0;
-    for (int q = 0; q < tk.nslots; ++q) acc += double(tk.src[e + q * tk.stride]);
+    int q = 0;
+    for (; q + 4 <= tk.nslots; q += 4) {
+      T v[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[j] = tk.src[e + (q + j) * tk.stride];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc += double(v[j]);
+    }
+    for (; q < tk.nslots; ++q) acc += double(tk.src[e + q * tk.stride]);
     tk.dst[e] = T(acc);
   }
 }
@@ -428,8 +438,13 @@ template <typename T>
 void launch_sum_slots(const SumTask<T> *tasks, int ntasks, long long max_len, cudaStream_t s) {
   if (ntasks <= 0 || max_len <= 0) return;
   // grid.y is at most 65535: merged batches can hold more tasks than that
+  // about 16 CTAs per SM in all (each thread takes several elements): a grid
+  // of one CTA per 256 elements of every task was ~34 k short CTAs at
+  // N = 262144, bound by how fast CTAs start
+  const long long per_task = std::max<long long>(1, 2368 / std::max(1, ntasks));
   for (int t0 = 0; t0 < ntasks; t0 += 65535) {
-    dim3 grid((unsigned)std::min<long long>(cdiv<long long>(max_len, kThreads), 4096),
+    dim3 grid((unsigned)std::min<long long>(cdiv<long long>(max_len, kThreads),
+                                            std::min<long long>(per_task, 4096)),
               std::min(65535, ntasks - t0));
     sum_slots_kernel<T><<<grid, kThreads, 0, s>>>(tasks + t0);
     HODLR_LAUNCH_CHECK();
