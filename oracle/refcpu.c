@@ -32,6 +32,13 @@
  * path needs an oracle for: ref_hodlr_matvec (A x from D, U, V) and the dense
  * assembly ref_hodlr_dense.
  *
+ * Parity unpinned: the reference cannot be built or run without Legion, and
+ * its known-answer test (test/single_launch.cc:20-75) stores no expected
+ * numbers (it compares against a dense solve), so this oracle is checked
+ * against tests/golden/, which tests/golden/make_golden.py computes from the
+ * same known-answer inputs with numpy alone, not against outputs of the
+ * reference itself.
+ *
  * Arithmetic is LAPACK/BLAS dgesv_/dgemm_ as in the reference
  * (include/core/lapack_blas.h:28-55).  The reference links an unpinned system
  * netlib/MKL LAPACK; here the same Fortran-ABI routines are resolved at run
